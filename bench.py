@@ -1,0 +1,358 @@
+"""Benchmark: 2D magnetic rotor, HLLD + PLM(MC) + SSP-RK3 + CT, zone-updates/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--n 2048] [--precision fp64|fp64_exact]
+
+One step is one full SSP-RK3 step (three stages, each: x and y sweeps, corner
+EMF + update, sync) of the periodic tapered rotor on [0,1]^2 at n^2 cells,
+preceded by the on-device CFL time step, with the state resident in HBM
+(1.5 GB at 2048^2, far above the 126 MB L2, so no flush is needed).  The
+line printed by rank 0 also carries the end-to-end rate through the public
+API with the state copied host -> device and back every step, the roofline
+of the dominant kernel (the fused sweep), the CPU baseline (the C oracle on
+the host cores) and the SM clocks sampled during the timed region.
+
+N > 1 (torchrun): every rank advances its own rotor replica (the reference
+path has no domain decomposition; replicas only) and the rate is the sum
+over ranks timed by the slowest rank.
+
+``--impl reference`` times the CPU oracle (a C restatement of the
+reference's FP64 path) on the host cores with all threads, one RK3 step of
+the same rotor at 512^2 per step as a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PROBLEM = "rotor_tapered"
+WORKLOAD = "magnetic rotor 2D, periodic [0,1]^2, gamma 5/3, HLLD + PLM(MC, Wv) + SSP-RK3 + CT"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_exact"])
+    ap.add_argument("--cfl", type=float, default=0.4)
+    ap.add_argument("--cpu-n", type=int, default=512, help="grid of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh)["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ── clocks sampled during the timed region ───────────────────────────────────
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ── CPU baseline: the oracle on the host cores ───────────────────────────────
+
+def cpu_sample(n: int, steps: int, threads: int):
+    """zone-updates/s of the oracle's RK3 step on the rotor at n^2."""
+    from oracle import oracle
+    from hlld_ai_b200.physics.initial_data2d import b_from_potential, initial_prims
+    from hlld_ai_b200.physics.state import EVOLVED_KEYS, PRIM_KEYS
+
+    oracle.set_threads(threads)
+    g, eos, prims, Az, spec = initial_prims(PROBLEM, n, 2, "cpu")
+    prims = {k: v.contiguous().numpy().copy() for k, v in prims.items()}
+    Bxf, Byf = b_from_potential(Az, g.dx, g.dy)
+    cons = oracle.prim_to_cons(prims)
+    st = {"cons": {k: cons[k].copy() for k in EVOLVED_KEYS},
+          "Bxf": Bxf.contiguous().numpy().copy(), "Byf": Byf.contiguous().numpy().copy(),
+          "prims": {k: prims[k].copy() for k in PRIM_KEYS}}
+    og = oracle.Grid2DSpec(n, n, 2, g.dx, g.dy, *spec["bc"], "mc", "hlld", spec["gamma"])
+    oracle.sync_state(og, st)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        dt = oracle.compute_dt_2d(og, st["prims"], 0.4)
+        oracle.rk_step_ct(og, st, dt, "rk3")
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    cpu_sample(a.cpu_n, max(1, a.warmup), threads)  # warm-up
+    times = cpu_sample(a.cpu_n, a.steps, threads)
+    zu = a.cpu_n * a.cpu_n
+    value = zu * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": a.n, "sample_n": a.cpu_n,
+                   "l2": "inputs exceed L2"},
+        "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": threads,
+                         "kind": "port",
+                         "sample": f"one RK3 step of the same rotor at {a.cpu_n}^2 per step "
+                                   f"({zu} zone-updates), C oracle, {threads} threads"},
+        "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ── our arm ──────────────────────────────────────────────────────────────────
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    import hlld_ai_b200 as H
+    from hlld_ai_b200 import _lib
+    from hlld_ai_b200.physics.state import EVOLVED_KEYS, PRIM_KEYS
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev,
+                                timeout=__import__("datetime").timedelta(seconds=300))
+
+    g, eos, st, spec = H.setup_problem(PROBLEM, a.n, limiter="mc", device=dev,
+                                       precision=a.precision)
+    stepper = H.Stepper2D(g, eos, bc_x=spec["bc"][0], bc_y=spec["bc"][1], flux_fn="hlld",
+                          limiter="mc", precision=a.precision)
+    s = stepper._struct(st)
+    gc = stepper.gc
+    L = _lib.lib()
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    # component buffers of the instrumented step (same kernels as hlld_rk_step_ct)
+    nfx, nfy = (g.nxt + 1) * g.nyt, g.nxt * (g.nyt + 1)
+    f64 = dict(dtype=torch.float64, device=dev)
+    Fx = [torch.empty(nfx, **f64) for _ in range(7)]
+    Fy = [torch.empty(nfy, **f64) for _ in range(7)]
+    Ez = torch.empty((g.nxt + 1) * (g.nyt + 1), **f64)
+    U0 = [torch.empty(g.nxt * g.nyt, **f64) for _ in range(6)]
+    Bx0, By0 = torch.empty(nfx, **f64), torch.empty(nfy, **f64)
+    diag = torch.zeros(ctypes.sizeof(_lib.StepDiag), dtype=torch.uint8, device=dev)
+    fd_off = ctypes.sizeof(_lib.FluxDiag)
+    pFx, pFy, pU0 = _lib.ptr_array(Fx), _lib.ptr_array(Fy), _lib.ptr_array(U0)
+    dt = stepper.dt_buf
+    sweep_events = []
+
+    def step(record=False):
+        stepper.compute_dt(st, a.cfl, out=dt)
+        for stage in range(3):
+            for axis, pF in ((0, pFx), (1, pFy)):
+                if record:
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                _lib.check(L.hlld_sweep2d(ctypes.byref(gc), ctypes.byref(s), axis, pF,
+                                          diag.data_ptr() + axis * fd_off, sh), "sweep2d")
+                if record:
+                    e1.record(stream)
+                    sweep_events.append((e0, e1))
+            _lib.check(L.hlld_ct_update2d(ctypes.byref(gc), ctypes.byref(s), pFx, pFy,
+                                          Ez.data_ptr(), pU0, Bx0.data_ptr(), By0.data_ptr(),
+                                          diag.data_ptr(), stage, 3, 0.0, dt.data_ptr(), sh),
+                       "ct_update2d")
+            _lib.check(L.hlld_sync_state(ctypes.byref(gc), ctypes.byref(s), None,
+                                         None, sh), "sync_state")
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(a.steps):
+        step(record=True)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        m = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        ms = float(m.item())
+    zones = g.nx * g.ny
+    value = world * zones * a.steps / (ms * 1e-3)
+    launches_per_step = 2 + 3 * 9  # speed + dt; per stage 2 sweeps, emf, update, 2 face ghosts, cons ghosts, c2p, prim ghosts
+
+    # roofline of the dominant kernel (fused sweep), timed inside the region
+    sweep_ms = [e0.elapsed_time(e1) for e0, e1 in sweep_events]
+    sweep_avg_s = 1e-3 * sum(sweep_ms) / len(sweep_ms)
+    faces = (nfx + nfy) / 2.0
+    # algorithmic bytes per face: 6 primitives + 2 face-B words read per cell,
+    # 7 flux words written per face (FP64)
+    bytes_per_face = (8 + 7) * 8
+    achieved = bytes_per_face * faces / sweep_avg_s / 1e9
+    peak, peak_kind = peaks()
+    sweep_share = sum(sweep_ms) / ms
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not a.no_e2e:
+        host = {("cons", k): torch.empty_like(st.cons[k], device="cpu").pin_memory() for k in EVOLVED_KEYS}
+        host.update({("prims", k): torch.empty_like(st.prims[k], device="cpu").pin_memory() for k in PRIM_KEYS})
+        host[("Bxf", None)] = torch.empty_like(st.Bxf, device="cpu").pin_memory()
+        host[("Byf", None)] = torch.empty_like(st.Byf, device="cpu").pin_memory()
+
+        def dev_tensor(kind, k):
+            return st.cons[k] if kind == "cons" else st.prims[k] if kind == "prims" else getattr(st, kind)
+
+        for (kind, k), h in host.items():
+            h.copy_(dev_tensor(kind, k))
+        nbytes = sum(h.numel() * h.element_size() for h in host.values())
+        ke = max(2, min(a.steps, 5))
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ke):
+            for (kind, k), h in host.items():
+                dev_tensor(kind, k).copy_(h, non_blocking=True)
+            stepper.step(st, stepper.compute_dt(st, a.cfl), "rk3")
+            for (kind, k), h in host.items():
+                h.copy_(dev_tensor(kind, k), non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            m = torch.tensor([ems], dtype=torch.float64, device=dev)
+            dist.all_reduce(m, op=dist.ReduceOp.MAX)
+            ems = float(m.item())
+        e2e = {"value": world * zones * ke / (ems * 1e-3), "unit": "zone-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "steps": ke, "path": "Stepper2D.step + compute_dt with pinned host state"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cpu_sample(a.cpu_n, 1, threads)
+        times = cpu_sample(a.cpu_n, 3, threads)
+        cpu = {"value": a.cpu_n ** 2 * len(times) / sum(times), "unit": "zone-updates/s",
+               "cores": threads, "kind": "port",
+               "sample": f"3 RK3 steps of the same rotor at {a.cpu_n}^2 (C oracle, {threads} threads)"}
+
+    if rank == 0:
+        line = {
+            "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": a.n, "precision": a.precision,
+                       "parallelism": f"replicas x{world}", "cfl": a.cfl,
+                       "l2": "inputs exceed L2 (state 1.5 GB at 2048^2), no flush"},
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * a.steps,
+            "roofline": {"bound": "hbm", "kernel": "sweep_kernel (x and y)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "bytes_per_face": bytes_per_face,
+                         "avg_launch_ms": sweep_avg_s * 1e3, "share_of_step": sweep_share},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,273 @@
+// extern "C" entry points of libhlld_b200.so (declared in include/hlld_b200.h):
+// argument checks, scratch layout and dispatch to the arithmetic variant.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "variants.h"
+
+namespace {
+
+thread_local char g_detail[512] = "";
+
+int fail(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_detail, sizeof g_detail, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+// launch errors only (a kernel's own faults surface at the next sync)
+int check_launch(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(HLLD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return HLLD_OK;
+}
+
+bool fp64_precision(int precision) {
+    return precision == HLLD_FP64 || precision == HLLD_FP64_EXACT;
+}
+
+int check_grid(const hlld_grid2d_t *g) {
+    if (!g) return fail(HLLD_ERR_INVALID, "grid is NULL");
+    if (g->nx < 1 || g->ny < 1) return fail(HLLD_ERR_INVALID, "nx, ny must be >= 1");
+    if (g->ng < 1) return fail(HLLD_ERR_INVALID, "ng must be >= 1");
+    if (g->nx <= g->ng || g->ny <= g->ng)
+        return fail(HLLD_ERR_INVALID, "nx and ny must exceed ng (periodic ghost sources)");
+    if ((int64_t)(g->nx + 2 * g->ng + 1) * (g->ny + 2 * g->ng + 1) > (int64_t)1 << 31)
+        return fail(HLLD_ERR_INVALID, "grid too large for 32-bit face indexing");
+    if (g->bc_x < 0 || g->bc_x > 1 || g->bc_y < 0 || g->bc_y > 1)
+        return fail(HLLD_ERR_INVALID, "bc must be HLLD_BC_OUTFLOW or HLLD_BC_PERIODIC");
+    if (g->limiter < 0 || g->limiter > HLLD_LIM_MP7) return fail(HLLD_ERR_INVALID, "bad limiter");
+    static const int need[6] = {1, 1, 1, 2, 2, 3};  // stencil half-width per limiter
+    if (g->ng < need[g->limiter])
+        return fail(HLLD_ERR_INVALID, "ng = %d is too narrow for the limiter (needs %d)", g->ng,
+                    need[g->limiter]);
+    if (g->solver != HLLD_SOLVER_HLLE && g->solver != HLLD_SOLVER_HLLD)
+        return fail(HLLD_ERR_INVALID, "solver must be HLLE or HLLD");
+    if (!(g->gamma > 1.0)) return fail(HLLD_ERR_INVALID, "gamma must be > 1");
+    if (!(g->dx > 0.0) || !(g->dy > 0.0)) return fail(HLLD_ERR_INVALID, "dx, dy must be > 0");
+    if (!fp64_precision(g->precision))
+        return fail(HLLD_ERR_UNSUPPORTED, "precision %d not available for the 2D step", g->precision);
+    return HLLD_OK;
+}
+
+int check_state(const hlld_state2d_t *s) {
+    if (!s) return fail(HLLD_ERR_INVALID, "state is NULL");
+    for (int k = 0; k < 6; ++k)
+        if (!s->cons[k]) return fail(HLLD_ERR_INVALID, "state.cons[%d] is NULL", k);
+    for (int k = 0; k < 9; ++k)
+        if (!s->prims[k]) return fail(HLLD_ERR_INVALID, "state.prims[%d] is NULL", k);
+    if (!s->Bxf || !s->Byf) return fail(HLLD_ERR_INVALID, "state faces are NULL");
+    return HLLD_OK;
+}
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+// scratch layout of one 2D step; returns the byte count and fills sc when base != NULL
+size_t layout_scratch(const hlld_grid2d_t *g, char *base, hlld::Scratch2D *sc) {
+    const size_t nxt = g->nx + 2 * g->ng, nyt = g->ny + 2 * g->ng;
+    const size_t nfx = (nxt + 1) * nyt, nfy = nxt * (nyt + 1), ncr = (nxt + 1) * (nyt + 1),
+                 nc = nxt * nyt;
+    size_t off = 0;
+    auto take = [&](size_t count) -> double * {
+        double *p = base ? (double *)(base + off) : nullptr;
+        off += align_up(count * sizeof(double));
+        return p;
+    };
+    hlld::Scratch2D s{};
+    for (int k = 0; k < 7; ++k) s.Fx[k] = take(nfx);
+    for (int k = 0; k < 7; ++k) s.Fy[k] = take(nfy);
+    s.Ez = take(ncr);
+    for (int k = 0; k < 6; ++k) s.U0[k] = take(nc);
+    s.Bx0 = take(nfx);
+    s.By0 = take(nfy);
+    s.diag = base ? (hlld_step_diag_t *)(base + off) : nullptr;
+    off += align_up(sizeof(hlld_step_diag_t));
+    if (sc) *sc = s;
+    return off;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hlld_version(void) { return 1; }
+
+const char *hlld_error_string(int code) {
+    switch (code) {
+    case HLLD_OK: return "ok";
+    case HLLD_ERR_INVALID: return "invalid argument";
+    case HLLD_ERR_CUDA: return "CUDA error";
+    case HLLD_ERR_UNSUPPORTED: return "unsupported";
+    case HLLD_ERR_SCRATCH: return "scratch buffer too small";
+    default: return "unknown error";
+    }
+}
+
+const char *hlld_last_error_detail(void) { return g_detail; }
+
+int hlld_prim_to_cons(int64_t n, const void *const *prim, int precision, void *const *cons,
+                      void *stream) {
+    if (n < 0 || !prim || !cons) return fail(HLLD_ERR_INVALID, "bad arguments");
+    if (!fp64_precision(precision)) return fail(HLLD_ERR_UNSUPPORTED, "precision %d", precision);
+    if (n == 0) return HLLD_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == HLLD_FP64_EXACT) hlld::v_exact::launch_prim_to_cons(n, prim, cons, st);
+    else hlld::v_fp64::launch_prim_to_cons(n, prim, cons, st);
+    return check_launch("prim_to_cons");
+}
+
+int hlld_cons_to_prim(int64_t n, const void *const *cons, double gamma, double atmo_rho,
+                      double atmo_eps, int precision, void *const *prim, uint8_t *status,
+                      void *stream) {
+    if (n < 0 || !cons || !prim) return fail(HLLD_ERR_INVALID, "bad arguments");
+    if (!(gamma > 1.0)) return fail(HLLD_ERR_INVALID, "gamma must be > 1");
+    if (!fp64_precision(precision)) return fail(HLLD_ERR_UNSUPPORTED, "precision %d", precision);
+    if (n == 0) return HLLD_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == HLLD_FP64_EXACT)
+        hlld::v_exact::launch_cons_to_prim(n, cons, gamma, atmo_rho, atmo_eps, prim, status, st);
+    else
+        hlld::v_fp64::launch_cons_to_prim(n, cons, gamma, atmo_rho, atmo_eps, prim, status, st);
+    return check_launch("cons_to_prim");
+}
+
+int hlld_riemann_faces(int64_t n, const void *const *sL, const void *const *sR, int idir,
+                       int solver, double gamma, int precision, void *const *F, void *const *U,
+                       void *pstar, int32_t *err, int32_t *iters, uint8_t *flags,
+                       hlld_flux_diag_t *diag, void *stream) {
+    if (n < 0 || !sL || !sR || !F || !pstar) return fail(HLLD_ERR_INVALID, "bad arguments");
+    if (idir < 0 || idir > 2) return fail(HLLD_ERR_INVALID, "idir must be 0, 1 or 2");
+    if (solver != HLLD_SOLVER_HLLE && solver != HLLD_SOLVER_HLLD)
+        return fail(HLLD_ERR_INVALID, "solver must be HLLE or HLLD");
+    if (!(gamma > 1.0)) return fail(HLLD_ERR_INVALID, "gamma must be > 1");
+    if (!fp64_precision(precision)) return fail(HLLD_ERR_UNSUPPORTED, "precision %d", precision);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (diag && cudaMemsetAsync(diag, 0, sizeof(hlld_flux_diag_t), st) != cudaSuccess)
+        return check_launch("riemann_faces diag reset");
+    if (n == 0) return HLLD_OK;
+    if (precision == HLLD_FP64_EXACT)
+        hlld::v_exact::launch_riemann_faces(n, sL, sR, idir, solver, gamma, F, U, pstar, err, iters,
+                                            flags, diag, st);
+    else
+        hlld::v_fp64::launch_riemann_faces(n, sL, sR, idir, solver, gamma, F, U, pstar, err, iters,
+                                           flags, diag, st);
+    return check_launch("riemann_faces");
+}
+
+int hlld_step2d_scratch_bytes(const hlld_grid2d_t *g, size_t *bytes) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (!bytes) return fail(HLLD_ERR_INVALID, "bytes is NULL");
+    *bytes = layout_scratch(g, nullptr, nullptr);
+    return HLLD_OK;
+}
+
+int hlld_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scratch,
+                    size_t scratch_bytes, double dt_host, const double *dt_dev, int scheme,
+                    hlld_step_diag_t *diag, void *stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_state(s))) return rc;
+    if (scheme != 2 && scheme != 3) return fail(HLLD_ERR_INVALID, "scheme must be 2 or 3");
+    if (!scratch) return fail(HLLD_ERR_INVALID, "scratch is NULL");
+    if ((uintptr_t)scratch % kAlign) return fail(HLLD_ERR_INVALID, "scratch must be 256-byte aligned");
+    hlld::Scratch2D sc;
+    size_t need = layout_scratch(g, (char *)scratch, &sc);
+    if (scratch_bytes < need)
+        return fail(HLLD_ERR_SCRATCH, "scratch has %zu bytes, the step needs %zu", scratch_bytes, need);
+    if (!dt_dev && !(dt_host == dt_host)) return fail(HLLD_ERR_INVALID, "dt is NaN");
+    hlld_step_diag_t *d = diag ? diag : sc.diag;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->precision == HLLD_FP64_EXACT)
+        hlld::v_exact::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
+    else
+        hlld::v_fp64::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
+    return check_launch("rk_step_ct");
+}
+
+int hlld_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
+                    hlld_step_diag_t *diag, void *stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_state(s))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (diag && cudaMemsetAsync(diag, 0, sizeof(hlld_step_diag_t), st) != cudaSuccess)
+        return check_launch("sync_state diag reset");
+    if (g->precision == HLLD_FP64_EXACT)
+        hlld::v_exact::launch_sync_state(g, s, status, diag, st);
+    else
+        hlld::v_fp64::launch_sync_state(g, s, status, diag, st);
+    return check_launch("sync_state");
+}
+
+int hlld_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
+                 hlld_flux_diag_t *diag, void *stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_state(s))) return rc;
+    if (axis != 0 && axis != 1) return fail(HLLD_ERR_INVALID, "axis must be 0 or 1");
+    if (!F || !diag) return fail(HLLD_ERR_INVALID, "F and diag are required");
+    for (int k = 0; k < 7; ++k)
+        if (!F[k]) return fail(HLLD_ERR_INVALID, "F[%d] is NULL", k);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(diag, 0, sizeof(hlld_flux_diag_t), st) != cudaSuccess)
+        return check_launch("sweep2d diag reset");
+    if (g->precision == HLLD_FP64_EXACT)
+        hlld::v_exact::launch_sweep2d(g, s, axis, (double *const *)F, diag, st);
+    else
+        hlld::v_fp64::launch_sweep2d(g, s, axis, (double *const *)F, diag, st);
+    return check_launch("sweep2d");
+}
+
+int hlld_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *const *Fx,
+                     void *const *Fy, void *Ez, void *const *U0, void *Bx0, void *By0,
+                     const hlld_step_diag_t *diag, int stage, int scheme, double dt_host,
+                     const double *dt_dev, void *stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_state(s))) return rc;
+    if (scheme != 2 && scheme != 3) return fail(HLLD_ERR_INVALID, "scheme must be 2 or 3");
+    if (stage < 0 || stage >= scheme) return fail(HLLD_ERR_INVALID, "stage out of range");
+    if (!Fx || !Fy || !Ez || !U0 || !Bx0 || !By0 || !diag)
+        return fail(HLLD_ERR_INVALID, "NULL array argument");
+    hlld::Scratch2D sc{};
+    for (int k = 0; k < 7; ++k) {
+        sc.Fx[k] = (double *)Fx[k];
+        sc.Fy[k] = (double *)Fy[k];
+        if (!sc.Fx[k] || !sc.Fy[k]) return fail(HLLD_ERR_INVALID, "flux array %d is NULL", k);
+    }
+    for (int k = 0; k < 6; ++k) {
+        sc.U0[k] = (double *)U0[k];
+        if (!sc.U0[k]) return fail(HLLD_ERR_INVALID, "U0[%d] is NULL", k);
+    }
+    sc.Ez = (double *)Ez;
+    sc.Bx0 = (double *)Bx0;
+    sc.By0 = (double *)By0;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->precision == HLLD_FP64_EXACT)
+        hlld::v_exact::launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
+    else
+        hlld::v_fp64::launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
+    return check_launch("ct_update2d");
+}
+
+int hlld_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,
+                       double *dt_dev, unsigned long long *work, void *stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_state(s))) return rc;
+    if (!dt_dev || !work) return fail(HLLD_ERR_INVALID, "dt_dev and work must be device pointers");
+    if (!(cfl > 0.0)) return fail(HLLD_ERR_INVALID, "cfl must be > 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->precision == HLLD_FP64_EXACT)
+        hlld::v_exact::launch_compute_dt_2d(g, s, cfl, dt_dev, work, st);
+    else
+        hlld::v_fp64::launch_compute_dt_2d(g, s, cfl, dt_dev, work, st);
+    return check_launch("compute_dt_2d");
+}
+
+}  // extern "C"

@@ -1,0 +1,1003 @@
+// Kernels of the SRMHD step, compiled once per arithmetic variant: this
+// header is included by a translation unit that defines HLLD_NS (the
+// variant's namespace) and is built with or without FMA contraction.
+//
+// Kernels:
+//   riemann_faces_kernel  flux_fn plugin on flattened faces (hlld.py:1005, :1202)
+//   c2p_kernel            conservative_to_primitive (c2p.py:313-363)
+//   p2c_kernel            primitive_to_conserved (hlld.py:185-217)
+//   sweep_kernel          one directional sweep of the 2D step, fused:
+//                         reconstruction + normal-B override + Riemann
+//                         solver + max|F_D| (sweep.py:30-119, reconstruction.py:272-338)
+//   ct_emf_kernel         Gardiner-Stone corner EMF (ct.py:44-177)
+//   ct_update_kernel      flux divergence + CT face update + RK combine
+//                         (sweep.py:122-135, ct.py:180-185, state.py:77-103)
+//   ghost_kernel          separable ghost fill (grid.py:93-143, :229-255)
+//   c2p_cells_kernel      cell-centred B + C2P of physical cells (driver2d.py:395-417)
+//   speed_kernel/dt_kernel compute_dt_2d (driver2d.py:251-281)
+#pragma once
+
+#ifndef HLLD_NS
+#error "define HLLD_NS before including kernels_impl.cuh"
+#endif
+
+#include "srmhd_phys.cuh"
+#include "variants.h"
+
+namespace hlld {
+namespace HLLD_NS {
+
+constexpr int kThreads = 128;
+
+// ── small utilities ──────────────────────────────────────────────────────
+
+// non-negative doubles order like their bit patterns; a NaN (sign cleared)
+// sorts above +inf, so atomicMax on the bits propagates it like torch's max
+__device__ __forceinline__ unsigned long long abs_bits(double x) {
+    return (unsigned long long)__double_as_longlong(fabs(x));
+}
+
+struct Counts {
+    unsigned long long v[9];  // slots [0, NS) are summed, [NS, NS + NM) maxed
+};
+
+// Block-reduce NS sum slots and NM max slots; thread 0 adds the sums to
+// dst[0..NS) and max-combines the maxima into dmax[0..NM).  Every thread of
+// the block must call it.
+template <int NS, int NM>
+__device__ __forceinline__ void block_accumulate(Counts c, unsigned long long *dst,
+                                                 unsigned long long *const *dmax) {
+    __shared__ unsigned long long sm[kThreads / 32][NS + NM];
+#pragma unroll
+    for (int k = 0; k < NS + NM; ++k) {
+        unsigned long long x = c.v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long y = __shfl_down_sync(0xffffffffu, x, o);
+            x = (k >= NS) ? (x > y ? x : y) : x + y;
+        }
+        c.v[k] = x;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NS + NM; ++k) sm[w][k] = c.v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s[NS + NM];
+#pragma unroll
+        for (int k = 0; k < NS + NM; ++k) s[k] = sm[0][k];
+        for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww)
+#pragma unroll
+            for (int k = 0; k < NS + NM; ++k)
+                s[k] = (k >= NS) ? (s[k] > sm[ww][k] ? s[k] : sm[ww][k]) : s[k] + sm[ww][k];
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+            if (s[k]) atomicAdd(dst + k, s[k]);
+#pragma unroll
+        for (int k = 0; k < NM; ++k)
+            if (s[NS + k]) atomicMax(dmax[k], s[NS + k]);
+    }
+}
+
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long x) {
+    __shared__ unsigned long long sm[kThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long y = __shfl_down_sync(0xffffffffu, x, o);
+        x = x > y ? x : y;
+    }
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm[w] = x;
+    __syncthreads();
+    unsigned long long r = 0;
+    if (threadIdx.x == 0) {
+        r = sm[0];
+        for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) r = r > sm[ww] ? r : sm[ww];
+    }
+    return r;
+}
+
+// ── reconstruction (reconstruction.py) ───────────────────────────────────
+
+template <typename T> __device__ __forceinline__ T minmod(T a, T b) {
+    return (a * b > T(0)) ? ((fabs(a) < fabs(b)) ? a : b) : T(0);
+}
+template <typename T> __device__ __forceinline__ T mc_lim(T a, T b) {
+    T c = T(0.5) * (a + b);
+    return (a * b > T(0)) ? tsign(c) * tmin(T(2) * fabs(a), tmin(T(2) * fabs(b), fabs(c))) : T(0);
+}
+// reconstruction.py:111-128
+template <typename T> __device__ __forceinline__ T weno5z(T vm2, T vm1, T v0, T vp1, T vp2) {
+    T p0 = (T(2) * vm2 - T(7) * vm1 + T(11) * v0) / T(6);
+    T p1 = (-vm1 + T(5) * v0 + T(2) * vp1) / T(6);
+    T p2 = (T(2) * v0 + T(5) * vp1 - vp2) / T(6);
+    const T c1 = T(13.0 / 12.0), c2 = T(0.25);
+    T t = vm2 - T(2) * vm1 + v0, u = vm2 - T(4) * vm1 + T(3) * v0;
+    T b0 = c1 * (t * t) + c2 * (u * u);
+    t = vm1 - T(2) * v0 + vp1;
+    u = vm1 - vp1;
+    T b1 = c1 * (t * t) + c2 * (u * u);
+    t = v0 - T(2) * vp1 + vp2;
+    u = T(3) * v0 - T(4) * vp1 + vp2;
+    T b2 = c1 * (t * t) + c2 * (u * u);
+    T tau5 = fabs(b0 - b2);
+    const T eps = K<T>::weno_eps;
+    T r0 = tau5 / (b0 + eps), r1 = tau5 / (b1 + eps), r2 = tau5 / (b2 + eps);
+    T a0 = T(0.1) * (T(1) + r0 * r0);
+    T a1 = T(0.6) * (T(1) + r1 * r1);
+    T a2 = T(0.3) * (T(1) + r2 * r2);
+    return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
+}
+// reconstruction.py:136-162
+template <typename T>
+__device__ __forceinline__ T mp_limit(T vl, T vm2, T vm1, T v0, T vp1, T vp2) {
+    const T alpha = T(4);
+    T vmp = v0 + minmod(vp1 - v0, alpha * (v0 - vm1));
+    bool need = (vl - v0) * (vl - vmp) > K<T>::mp_eps;
+    if (!need) return vl;
+    T d_m1 = vm2 - T(2) * vm1 + v0;
+    T d_0 = vm1 - T(2) * v0 + vp1;
+    T d_p1 = v0 - T(2) * vp1 + vp2;
+    T dm4_p = minmod(minmod(T(4) * d_0 - d_p1, T(4) * d_p1 - d_0), minmod(d_0, d_p1));
+    T dm4_m = minmod(minmod(T(4) * d_m1 - d_0, T(4) * d_0 - d_m1), minmod(d_m1, d_0));
+    T v_ul = v0 + alpha * (v0 - vm1);
+    T v_av = T(0.5) * (v0 + vp1);
+    T v_md = v_av - T(0.5) * dm4_p;
+    T v_lc = v0 + T(0.5) * (v0 - vm1) + T(4.0 / 3.0) * dm4_m;
+    T vmin = tmax(tmin(tmin(v0, vp1), v_md), tmin(tmin(v0, v_ul), v_lc));
+    T vmax = tmin(tmax(tmax(v0, vp1), v_md), tmax(tmax(v0, v_ul), v_lc));
+    return vl + minmod(vmin - vl, vmax - vl);
+}
+template <typename T> __device__ __forceinline__ T mp5(T vm2, T vm1, T v0, T vp1, T vp2) {
+    T vl = (T(2) * vm2 - T(13) * vm1 + T(47) * v0 + T(27) * vp1 - T(3) * vp2) / T(60);
+    return mp_limit(vl, vm2, vm1, v0, vp1, vp2);
+}
+template <typename T>
+__device__ __forceinline__ T mp7(T vm3, T vm2, T vm1, T v0, T vp1, T vp2, T vp3) {
+    T vl = (T(-3) * vm3 + T(25) * vm2 - T(101) * vm1 + T(319) * v0 + T(214) * vp1 - T(38) * vp2 +
+            T(4) * vp3) /
+           T(420);
+    return mp_limit(vl, vm2, vm1, v0, vp1, vp2);
+}
+
+template <int LIM> struct Stencil { static constexpr int S = 1; };
+template <> struct Stencil<HLLD_LIM_PCM> { static constexpr int S = 1; };
+template <> struct Stencil<HLLD_LIM_WENO5Z> { static constexpr int S = 2; };
+template <> struct Stencil<HLLD_LIM_MP5> { static constexpr int S = 2; };
+template <> struct Stencil<HLLD_LIM_MP7> { static constexpr int S = 3; };
+
+// Edge value of cell c (window index M, i.e. cell c = base + M) toward
+// the right (RIGHT = true: value at c+1/2) or the left (c-1/2), for one line
+// of n cells; reconstruction.py:182-264.
+template <int LIM, bool RIGHT, int M, typename T>
+__device__ __forceinline__ T cell_edge(const T *w, int c, int n) {
+    if (LIM == HLLD_LIM_PCM) return RIGHT ? w[M] + T(0.5) * T(0) : w[M] - T(0.5) * T(0);
+    constexpr int HW = (LIM == HLLD_LIM_WENO5Z || LIM == HLLD_LIM_MP5) ? 2 : (LIM == HLLD_LIM_MP7 ? 3 : 0);
+    if (HW > 0 && n > 2 * HW && c >= HW && c < n - HW) {
+        if (LIM == HLLD_LIM_WENO5Z) {
+            return RIGHT ? weno5z(w[M - 2], w[M - 1], w[M], w[M + 1], w[M + 2])
+                         : weno5z(w[M + 2], w[M + 1], w[M], w[M - 1], w[M - 2]);
+        } else if (LIM == HLLD_LIM_MP5) {
+            return RIGHT ? mp5(w[M - 2], w[M - 1], w[M], w[M + 1], w[M + 2])
+                         : mp5(w[M + 2], w[M + 1], w[M], w[M - 1], w[M - 2]);
+        } else {
+            if constexpr (HW == 3)
+                return RIGHT ? mp7(w[M - 3], w[M - 2], w[M - 1], w[M], w[M + 1], w[M + 2], w[M + 3])
+                             : mp7(w[M + 3], w[M + 2], w[M + 1], w[M], w[M - 1], w[M - 2], w[M - 3]);
+        }
+    }
+    T slope = T(0);
+    if (c >= 1 && c <= n - 2) {
+        T a = w[M] - w[M - 1];
+        T b = w[M + 1] - w[M];
+        slope = (LIM == HLLD_LIM_MINMOD) ? minmod(a, b) : mc_lim(a, b);
+    }
+    return RIGHT ? w[M] + T(0.5) * slope : w[M] - T(0.5) * slope;
+}
+
+// ── per-element kernels (flattened plugin API) ───────────────────────────
+
+struct FacesParams {
+    int64_t n;
+    const double *sL[9];
+    const double *sR[9];
+    double *F[8];
+    double *U[8];
+    double *pstar;
+    int32_t *err;
+    int32_t *iters;
+    uint8_t *flags;
+    hlld_flux_diag_t *diag;
+    double gamma;
+};
+
+template <int IDIR, int SOLVER>
+__global__ void __launch_bounds__(kThreads) riemann_faces_kernel(const FacesParams p) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    Counts c = {};
+    bool live = e < p.n;
+    if (live) {
+        double PL[NPRIM], PR[NPRIM];
+#pragma unroll
+        for (int k = 0; k < NPRIM; ++k) {
+            PL[k] = p.sL[k][e];
+            PR[k] = p.sR[k][e];
+        }
+        FaceOut<double> o;
+        bool want_u = p.U[0] != nullptr;
+        if (SOLVER == HLLD_SOLVER_HLLD)
+            hlld_face<IDIR, double>(PL, PR, p.gamma, want_u, o);
+        else
+            hlle_face<IDIR, double>(PL, PR, p.gamma, want_u, true, o);
+#pragma unroll
+        for (int k = 0; k < NCONS; ++k) p.F[k][e] = o.F[k];
+        if (want_u)
+#pragma unroll
+            for (int k = 0; k < NCONS; ++k) p.U[k][e] = o.U[k];
+        p.pstar[e] = o.pstar;
+        if (p.err) p.err[e] = o.err;
+        if (p.iters) p.iters[e] = o.iters;
+        if (p.flags) p.flags[e] = o.flags;
+        c.v[0] = 1;
+        c.v[1] = o.err > 0;
+        c.v[2] = (o.flags & RF_WAVE_ORDER_BAD) != 0;
+        c.v[3] = (o.flags & RF_BN_ZERO) != 0;
+        c.v[4] = (o.flags & RF_FAILED) != 0;
+        c.v[5] = (o.err == 0) ? (unsigned long long)o.iters : 0ull;
+        c.v[6] = o.err == 0;
+        c.v[7] = (unsigned long long)o.iters;
+        c.v[8] = abs_bits(o.F[C_D]);
+    }
+    if (p.diag) {
+        unsigned long long *mx[2] = {&p.diag->max_iters, &p.diag->fd_max_bits};
+        block_accumulate<7, 2>(c, &p.diag->n_faces, mx);
+    }
+}
+
+struct CellsParams {
+    int64_t n;
+    const double *in[9];
+    double *out[9];
+    uint8_t *status;
+    double gamma, atmo_rho, atmo_eps;
+};
+
+__global__ void __launch_bounds__(kThreads) c2p_kernel(const CellsParams p) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= p.n) return;
+    double C[NCONS], P[NPRIM];
+#pragma unroll
+    for (int k = 0; k < NCONS; ++k) C[k] = p.in[k][e];
+    uint8_t st = cons_to_prim<double>(C, p.gamma, p.atmo_rho, p.atmo_eps, P);
+#pragma unroll
+    for (int k = 0; k < NPRIM; ++k) p.out[k][e] = P[k];
+    if (p.status) p.status[e] = st;
+}
+
+__global__ void __launch_bounds__(kThreads) p2c_kernel(const CellsParams p) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= p.n) return;
+    double P[NPRIM], C[NCONS];
+#pragma unroll
+    for (int k = 0; k < NPRIM; ++k) P[k] = p.in[k][e];
+    prim_to_cons<double>(P, C);
+#pragma unroll
+    for (int k = 0; k < NCONS; ++k) p.out[k][e] = C[k];
+}
+
+// ── 2D step kernels ──────────────────────────────────────────────────────
+
+struct Grid {
+    int nx, ny, ng, nxt, nyt;
+    double dx, dy, gamma, atmo_rho;
+    int bc_x, bc_y;
+};
+
+// face flux slots of a sweep: the six evolved fluxes plus the transverse-B
+// flux that becomes the face EMF (ct.py:63-88)
+enum { F_D = 0, F_SX, F_SY, F_SZ, F_TAU, F_BZ, F_BT, NFLUX };
+
+struct SweepParams {
+    Grid g;
+    const double *rho, *p, *vx, *vy, *vz, *bz, *Bxf, *Byf;
+    double *F[NFLUX];
+    hlld_flux_diag_t *diag;
+};
+
+// One face of a directional sweep.  AXIS 0: faces (nxt+1, nyt), face f is
+// the lower-x face of cell (f, j).  AXIS 1: faces (nxt, nyt+1).
+template <int AXIS, int LIM, int SOLVER>
+__global__ void __launch_bounds__(kThreads) sweep_kernel(const SweepParams p) {
+    using T = double;
+    constexpr int S = Stencil<LIM>::S;
+    constexpr int NW = 2 * S + 2;
+    const Grid &g = p.g;
+    const int cols = AXIS == 0 ? g.nyt : g.nyt + 1;
+    const int rows = AXIS == 0 ? g.nxt + 1 : g.nxt;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    Counts cnt = {};
+    const bool live = e < (int64_t)rows * cols;
+    if (live) {
+        const int row = (int)(e / cols), col = (int)(e - (int64_t)row * cols);
+        const int f = AXIS == 0 ? row : col;   // face index along the sweep axis
+        const int tr = AXIS == 0 ? col : row;  // transverse index
+        const int n = AXIS == 0 ? g.nxt : g.nyt;
+        const int64_t cstride = AXIS == 0 ? g.nyt : 1;
+        const int64_t cbase = AXIS == 0 ? (int64_t)tr : (int64_t)tr * g.nyt;
+        // work variables (reconstruction.py:269): rho, p, W vx, W vy, W vz,
+        // transverse in-plane B (cell-centred from faces, ct.py:44-54), Bz
+        T L[7], R[7];
+        if (f == 0 || f == n) {
+            // outermost faces: the edge cell has zero slope in every scheme
+            const int c = f == 0 ? 0 : n - 1;
+            const int64_t ci = cbase + c * cstride;
+            T vx = p.vx[ci], vy = p.vy[ci], vz = p.vz[ci];
+            T v2 = vx * vx + vy * vy + vz * vz;
+            T W = T(1) / sqrt(clamp_lo(T(1) - v2, T(1e-14)));
+            T bt = AXIS == 0 ? T(0.5) * (p.Byf[(int64_t)c * (g.nyt + 1) + tr] + p.Byf[(int64_t)c * (g.nyt + 1) + tr + 1])
+                             : T(0.5) * (p.Bxf[(int64_t)tr * g.nyt + c] + p.Bxf[(int64_t)(tr + 1) * g.nyt + c]);
+            T q[7] = {p.rho[ci], p.p[ci], W * vx, W * vy, W * vz, bt, p.bz[ci]};
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                L[k] = q[k] + T(0.5) * T(0);
+                R[k] = q[k] - T(0.5) * T(0);
+            }
+        } else {
+            // window of cells f-1-S .. f+S (clamped; clamped entries are never
+            // read by the edge rules)
+            int cw[NW];
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                int c = f - 1 - S + k;
+                cw[k] = c < 0 ? 0 : (c > n - 1 ? n - 1 : c);
+            }
+            T Wf[NW];
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                const int64_t ci = cbase + cw[k] * cstride;
+                T vx = p.vx[ci], vy = p.vy[ci], vz = p.vz[ci];
+                T v2 = vx * vx + vy * vy + vz * vz;
+                Wf[k] = T(1) / sqrt(clamp_lo(T(1) - v2, T(1e-14)));
+            }
+            T pcmL[7], pcmR[7];
+#pragma unroll
+            for (int v = 0; v < 7; ++v) {
+                T w[NW];
+#pragma unroll
+                for (int k = 0; k < NW; ++k) {
+                    const int c = cw[k];
+                    const int64_t ci = cbase + c * cstride;
+                    T x;
+                    switch (v) {
+                    case 0: x = p.rho[ci]; break;
+                    case 1: x = p.p[ci]; break;
+                    case 2: x = Wf[k] * p.vx[ci]; break;
+                    case 3: x = Wf[k] * p.vy[ci]; break;
+                    case 4: x = Wf[k] * p.vz[ci]; break;
+                    case 5:
+                        x = AXIS == 0 ? T(0.5) * (p.Byf[(int64_t)c * (g.nyt + 1) + tr] + p.Byf[(int64_t)c * (g.nyt + 1) + tr + 1])
+                                      : T(0.5) * (p.Bxf[(int64_t)tr * g.nyt + c] + p.Bxf[(int64_t)(tr + 1) * g.nyt + c]);
+                        break;
+                    default: x = p.bz[ci]; break;
+                    }
+                    w[k] = x;
+                }
+                L[v] = cell_edge<LIM, true, S>(w, f - 1, n);
+                R[v] = cell_edge<LIM, false, S + 1>(w, f, n);
+                pcmL[v] = w[S];
+                pcmR[v] = w[S + 1];
+            }
+            if (LIM != HLLD_LIM_PCM) {
+                // positivity fallback to PCM (reconstruction.py:315-326)
+                bool bad = (L[0] <= T(1e-12)) || (R[0] <= T(1e-12)) || (L[1] <= T(1e-14)) ||
+                           (R[1] <= T(1e-14));
+                if (bad) {
+#pragma unroll
+                    for (int v = 0; v < 7; ++v) {
+                        L[v] = pcmL[v] + T(0.5) * T(0);
+                        R[v] = pcmR[v] - T(0.5) * T(0);
+                    }
+                }
+            }
+        }
+        // Wv -> v, floors, EOS-consistent eps (reconstruction.py:328-336); the
+        // normal field is the face value (sweep.py:82-89)
+        const T bn = AXIS == 0 ? p.Bxf[(int64_t)f * g.nyt + tr] : p.Byf[(int64_t)tr * (g.nyt + 1) + f];
+        T PL[NPRIM], PR[NPRIM];
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            T *q = side == 0 ? L : R;
+            T *P = side == 0 ? PL : PR;
+            T z2 = q[2] * q[2] + q[3] * q[3] + q[4] * q[4];
+            T fac = T(1) / sqrt(T(1) + z2);
+            P[P_VX] = q[2] * fac;
+            P[P_VY] = q[3] * fac;
+            P[P_VZ] = q[4] * fac;
+            P[P_RHO] = clamp_lo(q[0], T(1e-12));
+            P[P_P] = clamp_lo(q[1], T(1e-14));
+            P[P_EPS] = eos_eps(P[P_P], P[P_RHO], (T)g.gamma);
+            P[P_BX] = AXIS == 0 ? bn : q[5];
+            P[P_BY] = AXIS == 0 ? q[5] : bn;
+            P[P_BZ] = q[6];
+        }
+        FaceOut<T> o;
+        if (SOLVER == HLLD_SOLVER_HLLD)
+            hlld_face<AXIS, T>(PL, PR, (T)g.gamma, false, o);
+        else
+            hlle_face<AXIS, T>(PL, PR, (T)g.gamma, false, false, o);
+        const int64_t fi = e;
+        p.F[F_D][fi] = o.F[C_D];
+        p.F[F_SX][fi] = o.F[C_SX];
+        p.F[F_SY][fi] = o.F[C_SY];
+        p.F[F_SZ][fi] = o.F[C_SZ];
+        p.F[F_TAU][fi] = o.F[C_TAU];
+        p.F[F_BZ][fi] = o.F[C_BZ];
+        p.F[F_BT][fi] = AXIS == 0 ? o.F[C_BY] : o.F[C_BX];
+        cnt.v[0] = 1;
+        cnt.v[1] = o.err > 0;
+        cnt.v[2] = (o.flags & RF_WAVE_ORDER_BAD) != 0;
+        cnt.v[3] = (o.flags & RF_BN_ZERO) != 0;
+        cnt.v[4] = (o.flags & RF_FAILED) != 0;
+        cnt.v[5] = (o.err == 0) ? (unsigned long long)o.iters : 0ull;
+        cnt.v[6] = o.err == 0;
+        cnt.v[7] = (unsigned long long)o.iters;
+        // max |F_D| over the sweep, for the CT deadband (ct.py:114)
+        cnt.v[8] = abs_bits(o.F[C_D]);
+    }
+    unsigned long long *mx[2] = {&p.diag->max_iters, &p.diag->fd_max_bits};
+    block_accumulate<7, 2>(cnt, &p.diag->n_faces, mx);
+}
+
+// ct.py:96-116 with the sweep-global scale
+__device__ __forceinline__ double upwind_sign(double F, double scale) {
+    return (fabs(F) > 1e-9 * scale) ? tsign(F) : 0.0;
+}
+
+struct CtParams {
+    Grid g;
+    const double *vx, *vy, *Bxf, *Byf;
+    const double *FxD, *FyD, *FxBt, *FyBt;
+    const hlld_step_diag_t *diag;
+    int upwind;
+    double *Ez;
+};
+
+// cell-centred E^z = v^y B^x - v^x B^y from face-averaged B (ct.py:44-60)
+__device__ __forceinline__ double cell_emf(const CtParams &p, int i, int j) {
+    const int nyt = p.g.nyt;
+    double Bcx = 0.5 * (p.Bxf[(int64_t)i * nyt + j] + p.Bxf[(int64_t)(i + 1) * nyt + j]);
+    double Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
+    int64_t c = (int64_t)i * nyt + j;
+    return Bcx * p.vy[c] - Bcy * p.vx[c];
+}
+
+__global__ void __launch_bounds__(kThreads) ct_emf_kernel(const CtParams p) {
+    const int nxt = p.g.nxt, nyt = p.g.nyt;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)(nxt + 1) * (nyt + 1)) return;
+    const int i = (int)(e / (nyt + 1)), j = (int)(e - (int64_t)i * (nyt + 1));
+    double val = 0.0;
+    if (i >= 1 && i <= nxt - 1 && j >= 1 && j <= nyt - 1) {
+        // Efy (nxt, nyt+1) = +F^y(Bx); Efx (nxt+1, nyt) = -F^x(By)
+        double Ezyf = p.FyBt[(int64_t)i * (nyt + 1) + j];
+        double Ezyfm = p.FyBt[(int64_t)(i - 1) * (nyt + 1) + j];
+        double Ezxf = -p.FxBt[(int64_t)i * nyt + j];
+        double Ezxfm = -p.FxBt[(int64_t)i * nyt + j - 1];
+        double EzNE = cell_emf(p, i, j);
+        double EzNW = cell_emf(p, i - 1, j);
+        double EzSE = cell_emf(p, i, j - 1);
+        double EzSW = cell_emf(p, i - 1, j - 1);
+        double Eavg = 0.25 * ((Ezyf + Ezyfm) + (Ezxf + Ezxfm));
+        if (p.upwind) {
+            double sx = __longlong_as_double((long long)p.diag->sweep[0].fd_max_bits);
+            double sy = __longlong_as_double((long long)p.diag->sweep[1].fd_max_bits);
+            double Sx = upwind_sign(p.FxD[(int64_t)i * nyt + j], sx);
+            double Sxm = upwind_sign(p.FxD[(int64_t)i * nyt + j - 1], sx);
+            double dEdyN = (1.0 - Sx) * (EzNE - Ezyf) + (1.0 + Sx) * (EzNW - Ezyfm);
+            double dEdyS = (1.0 - Sxm) * (Ezyf - EzSE) + (1.0 + Sxm) * (Ezyfm - EzSW);
+            double dEdy = 0.125 * (dEdyS - dEdyN);
+            double Sy = upwind_sign(p.FyD[(int64_t)i * (nyt + 1) + j], sy);
+            double Sym = upwind_sign(p.FyD[(int64_t)(i - 1) * (nyt + 1) + j], sy);
+            double dEdxE = (1.0 - Sy) * (EzNE - Ezxf) + (1.0 + Sy) * (EzSE - Ezxfm);
+            double dEdxW = (1.0 - Sym) * (Ezxf - EzNW) + (1.0 + Sym) * (Ezxfm - EzSW);
+            double dEdx = 0.125 * (dEdxW - dEdxE);
+            val = Eavg + (dEdy + dEdx);
+        } else {
+            val = Eavg;
+        }
+    }
+    p.Ez[e] = val;
+}
+
+struct UpdateParams {
+    Grid g;
+    double *U[6];
+    double *U0[6];
+    double *Bxf, *Byf, *Bx0, *By0;
+    const double *Fx[6];
+    const double *Fy[6];
+    const double *Ez;
+    const double *dt_dev;
+    double dt_host;
+    double a, b, c;
+    int first_stage;
+};
+
+// flux divergence + CT face update + RK combine on the physical block and
+// its upper faces; a thread owns cell (i, j), face Bxf(i, j), face Byf(i, j)
+__global__ void __launch_bounds__(kThreads) ct_update_kernel(const UpdateParams p) {
+    const Grid &g = p.g;
+    const int nyt = g.nyt;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)(g.nx + 1) * (g.ny + 1)) return;
+    const int ii = (int)(e / (g.ny + 1)), jj = (int)(e - (int64_t)ii * (g.ny + 1));
+    const int i = g.ng + ii, j = g.ng + jj;
+    const double dt = p.dt_dev ? *p.dt_dev : p.dt_host;
+    const double w2 = p.c * dt;
+    if (ii < g.nx && jj < g.ny) {
+        const int64_t c = (int64_t)i * nyt + j;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            double rx = -(p.Fx[k][(int64_t)(i + 1) * nyt + j] - p.Fx[k][c]) / g.dx;
+            double ry = -(p.Fy[k][(int64_t)i * (nyt + 1) + j + 1] - p.Fy[k][(int64_t)i * (nyt + 1) + j]) / g.dy;
+            double L = rx + ry;
+            double u = p.U[k][c];
+            double u0;
+            if (p.first_stage) {
+                u0 = u;
+                p.U0[k][c] = u;
+            } else {
+                u0 = p.U0[k][c];
+            }
+            double v = p.a * u0;
+            v = v + p.b * u;
+            v = v + w2 * L;
+            p.U[k][c] = v;
+        }
+    }
+    if (jj < g.ny) {
+        const int64_t fx = (int64_t)i * nyt + j;
+        double dB = (p.Ez[(int64_t)i * (nyt + 1) + j] - p.Ez[(int64_t)i * (nyt + 1) + j + 1]) / g.dy;
+        double u = p.Bxf[fx];
+        double u0;
+        if (p.first_stage) {
+            u0 = u;
+            p.Bx0[fx] = u;
+        } else {
+            u0 = p.Bx0[fx];
+        }
+        double v = p.a * u0;
+        v = v + p.b * u;
+        v = v + w2 * dB;
+        p.Bxf[fx] = v;
+    }
+    if (ii < g.nx) {
+        const int64_t fy = (int64_t)i * (nyt + 1) + j;
+        double dB = (p.Ez[(int64_t)(i + 1) * (nyt + 1) + j] - p.Ez[(int64_t)i * (nyt + 1) + j]) / g.dx;
+        double u = p.Byf[fy];
+        double u0;
+        if (p.first_stage) {
+            u0 = u;
+            p.By0[fy] = u;
+        } else {
+            u0 = p.By0[fy];
+        }
+        double v = p.a * u0;
+        v = v + p.b * u;
+        v = v + w2 * dB;
+        p.Byf[fy] = v;
+    }
+}
+
+// ── ghost fill (grid.py:93-143) ──────────────────────────────────────────
+
+// source index of a cell-centred array along one axis (grid.py:93-113)
+__device__ __forceinline__ int bc_cc_src(int idx, int n, int ng, int kind) {
+    if (idx >= ng && idx < ng + n) return idx;
+    if (kind == HLLD_BC_OUTFLOW) return idx < ng ? ng : ng + n - 1;
+    return idx < ng ? idx + n : idx - n;
+}
+// source index of a face array along its normal axis (grid.py:116-143)
+__device__ __forceinline__ int bc_face_src(int idx, int n, int ng, int kind) {
+    if (kind == HLLD_BC_OUTFLOW) {
+        if (idx < ng) return ng;
+        if (idx > ng + n) return ng + n;
+        return idx;
+    }
+    if (idx == ng + n) return ng;  // the periodic seam collapses onto face ng
+    if (idx < ng) return idx + n;
+    if (idx > ng + n) return idx - n;
+    return idx;
+}
+
+struct GhostParams {
+    double *v[9];  // blockIdx.y selects the array
+    int n0, n1;    // array shape
+    int a0, b0, a1, b1;  // block never written (its entries are every source)
+    int n_ph0, n_ph1, ng;
+    int kind0, kind1;
+    int face0, face1;    // axis is the face-normal axis of this array
+};
+
+// Fills every entry outside [a0,b0) x [a1,b1) from its separable source;
+// all sources lie inside that block, so the fill is race free in place.
+__global__ void __launch_bounds__(kThreads) ghost_kernel(const GhostParams p) {
+    double *v = p.v[blockIdx.y];
+    const int in0 = p.b0 - p.a0, in1 = p.b1 - p.a1;
+    const int64_t nA = (int64_t)(p.n0 - in0) * p.n1;
+    const int64_t nB = (int64_t)in0 * (p.n1 - in1);
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nA + nB) return;
+    int r, c;
+    if (e < nA) {
+        int rr = (int)(e / p.n1);
+        c = (int)(e - (int64_t)rr * p.n1);
+        r = rr < p.a0 ? rr : rr + in0;
+    } else {
+        int64_t e2 = e - nA;
+        int w = p.n1 - in1;
+        int rr = (int)(e2 / w);
+        int cc = (int)(e2 - (int64_t)rr * w);
+        r = p.a0 + rr;
+        c = cc < p.a1 ? cc : cc + in1;
+    }
+    int sr = p.face0 ? bc_face_src(r, p.n_ph0, p.ng, p.kind0) : bc_cc_src(r, p.n_ph0, p.ng, p.kind0);
+    int sc = p.face1 ? bc_face_src(c, p.n_ph1, p.ng, p.kind1) : bc_cc_src(c, p.n_ph1, p.ng, p.kind1);
+    v[(int64_t)r * p.n1 + c] = v[(int64_t)sr * p.n1 + sc];
+}
+
+struct C2PCellsParams {
+    Grid g;
+    const double *U[6];
+    const double *Bxf, *Byf;
+    double *P[9];
+    uint8_t *status;
+    hlld_step_diag_t *diag;
+};
+
+// cell-centred B (ct.py:44-54) + C2P (c2p.py:313-363) of the physical cells
+__global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParams p) {
+    const Grid &g = p.g;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    Counts cnt = {};
+    if (e < (int64_t)g.nx * g.ny) {
+        const int i = g.ng + (int)(e / g.ny), j = g.ng + (int)(e % g.ny);
+        const int nyt = g.nyt;
+        const int64_t c = (int64_t)i * nyt + j;
+        double Bcx = 0.5 * (p.Bxf[c] + p.Bxf[(int64_t)(i + 1) * nyt + j]);
+        double Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
+        double C[NCONS] = {p.U[0][c], p.U[1][c], p.U[2][c], p.U[3][c], p.U[4][c], Bcx, Bcy, p.U[5][c]};
+        double P[NPRIM];
+        uint8_t st = cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P);
+#pragma unroll
+        for (int k = 0; k < NPRIM; ++k) p.P[k][c] = P[k];
+        if (p.status) p.status[c] = st;
+        cnt.v[0] = !(st & ST_CONVERGED);
+        cnt.v[1] = (st & ST_BISECTED) != 0;
+        cnt.v[2] = (st & ST_ATMO) != 0;
+        cnt.v[3] = !(st & ST_BRACKET_OK);
+    }
+    if (p.diag) block_accumulate<4, 0>(cnt, &p.diag->c2p_not_converged, nullptr);
+}
+
+struct SpeedParams {
+    Grid g;
+    const double *P[9];
+    unsigned long long *out;  // [2]
+};
+
+// max(|v_d| + c_f) over the physical cells (driver2d.py:260-279)
+__global__ void __launch_bounds__(kThreads) speed_kernel(const SpeedParams p) {
+    const Grid &g = p.g;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long mx = 0, my = 0;
+    if (e < (int64_t)g.nx * g.ny) {
+        const int i = g.ng + (int)(e / g.ny), j = g.ng + (int)(e % g.ny);
+        const int64_t c = (int64_t)i * g.nyt + j;
+        double rho = p.P[P_RHO][c], eps = p.P[P_EPS][c];
+        double vx = p.P[P_VX][c], vy = p.P[P_VY][c], vz = p.P[P_VZ][c];
+        double Bx = p.P[P_BX][c], By = p.P[P_BY][c], Bz = p.P[P_BZ][c];
+        double pr, cs2;
+        eos_press_cs2(eps, rho, g.gamma, pr, cs2);
+        double v2 = vx * vx + vy * vy + vz * vz;
+        double W = 1.0 / sqrt(clamp_lo(1.0 - v2, 1e-10));
+        double B2 = Bx * Bx + By * By + Bz * Bz;
+        double vdotB = vx * Bx + vy * By + vz * Bz;
+        double b2 = (B2 + vdotB * vdotB) / (W * W);
+        double h = 1.0 + eps + pr / rho;
+        double v02 = cs2 + (b2 / (rho * h + b2)) * (1.0 - cs2);
+        double cf = sqrt(clamp_hi(clamp_lo(v02, 0.0), 1.0));
+        mx = abs_bits(fabs(vx) + cf);
+        my = abs_bits(fabs(vy) + cf);
+    }
+    unsigned long long bx = block_max_u64(mx);
+    __syncthreads();
+    unsigned long long by = block_max_u64(my);
+    if (threadIdx.x == 0) {
+        if (bx) atomicMax(p.out, bx);
+        if (by) atomicMax(p.out + 1, by);
+    }
+}
+
+// dt = cfl / (sx/dx + sy/dy), with torch's `cfl / tensor` = reciprocal * cfl
+__global__ void dt_kernel(const unsigned long long *speeds, double dx, double dy, double cfl,
+                          double *dt) {
+    double mx = __longlong_as_double((long long)speeds[0]);
+    double my = __longlong_as_double((long long)speeds[1]);
+    if (isnan(mx) || isnan(my)) {
+        *dt = mx + my;
+        return;
+    }
+    double sx = clamp_lo(mx, 1e-14), sy = clamp_lo(my, 1e-14);
+    *dt = (1.0 / (sx / dx + sy / dy)) * cfl;
+}
+
+// ── host-side launchers of this variant ──────────────────────────────────
+
+static inline unsigned grid1d(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+template <int IDIR>
+static void launch_faces_idir(int solver, const FacesParams &fp, cudaStream_t st) {
+    unsigned nb = grid1d(fp.n);
+    if (solver == HLLD_SOLVER_HLLD)
+        riemann_faces_kernel<IDIR, HLLD_SOLVER_HLLD><<<nb, kThreads, 0, st>>>(fp);
+    else
+        riemann_faces_kernel<IDIR, HLLD_SOLVER_HLLE><<<nb, kThreads, 0, st>>>(fp);
+}
+
+void launch_riemann_faces(int64_t n, const void *const *sL, const void *const *sR, int idir,
+                          int solver, double gamma, void *const *F, void *const *U, void *pstar,
+                          int32_t *err, int32_t *iters, uint8_t *flags, hlld_flux_diag_t *diag,
+                          cudaStream_t st) {
+    FacesParams fp = {};
+    fp.n = n;
+    for (int k = 0; k < 9; ++k) {
+        fp.sL[k] = (const double *)sL[k];
+        fp.sR[k] = (const double *)sR[k];
+    }
+    for (int k = 0; k < 8; ++k) {
+        fp.F[k] = (double *)F[k];
+        fp.U[k] = U ? (double *)U[k] : nullptr;
+    }
+    fp.pstar = (double *)pstar;
+    fp.err = err;
+    fp.iters = iters;
+    fp.flags = flags;
+    fp.diag = diag;
+    fp.gamma = gamma;
+    if (idir == 0) launch_faces_idir<0>(solver, fp, st);
+    else if (idir == 1) launch_faces_idir<1>(solver, fp, st);
+    else launch_faces_idir<2>(solver, fp, st);
+}
+
+void launch_cons_to_prim(int64_t n, const void *const *cons, double gamma, double atmo_rho,
+                         double atmo_eps, void *const *prim, uint8_t *status, cudaStream_t st) {
+    CellsParams cp = {};
+    cp.n = n;
+    for (int k = 0; k < 8; ++k) cp.in[k] = (const double *)cons[k];
+    for (int k = 0; k < 9; ++k) cp.out[k] = (double *)prim[k];
+    cp.status = status;
+    cp.gamma = gamma;
+    cp.atmo_rho = atmo_rho;
+    cp.atmo_eps = atmo_eps;
+    c2p_kernel<<<grid1d(n), kThreads, 0, st>>>(cp);
+}
+
+void launch_prim_to_cons(int64_t n, const void *const *prim, void *const *cons, cudaStream_t st) {
+    CellsParams cp = {};
+    cp.n = n;
+    for (int k = 0; k < 9; ++k) cp.in[k] = (const double *)prim[k];
+    for (int k = 0; k < 8; ++k) cp.out[k] = (double *)cons[k];
+    p2c_kernel<<<grid1d(n), kThreads, 0, st>>>(cp);
+}
+
+static Grid make_grid(const hlld_grid2d_t *g) {
+    Grid G;
+    G.nx = g->nx;
+    G.ny = g->ny;
+    G.ng = g->ng;
+    G.nxt = g->nx + 2 * g->ng;
+    G.nyt = g->ny + 2 * g->ng;
+    G.dx = g->dx;
+    G.dy = g->dy;
+    G.gamma = g->gamma;
+    G.atmo_rho = g->atmo_rho;
+    G.bc_x = g->bc_x;
+    G.bc_y = g->bc_y;
+    return G;
+}
+
+template <int AXIS, int LIM>
+static void launch_sweep_lim(int solver, const SweepParams &sp, cudaStream_t st) {
+    const int64_t nf = AXIS == 0 ? (int64_t)(sp.g.nxt + 1) * sp.g.nyt : (int64_t)sp.g.nxt * (sp.g.nyt + 1);
+    if (solver == HLLD_SOLVER_HLLD)
+        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLD><<<grid1d(nf), kThreads, 0, st>>>(sp);
+    else
+        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLE><<<grid1d(nf), kThreads, 0, st>>>(sp);
+}
+
+template <int AXIS>
+static void launch_sweep(int limiter, int solver, const SweepParams &sp, cudaStream_t st) {
+    switch (limiter) {
+    case HLLD_LIM_PCM: launch_sweep_lim<AXIS, HLLD_LIM_PCM>(solver, sp, st); break;
+    case HLLD_LIM_MC: launch_sweep_lim<AXIS, HLLD_LIM_MC>(solver, sp, st); break;
+    case HLLD_LIM_MINMOD: launch_sweep_lim<AXIS, HLLD_LIM_MINMOD>(solver, sp, st); break;
+    case HLLD_LIM_WENO5Z: launch_sweep_lim<AXIS, HLLD_LIM_WENO5Z>(solver, sp, st); break;
+    case HLLD_LIM_MP5: launch_sweep_lim<AXIS, HLLD_LIM_MP5>(solver, sp, st); break;
+    default: launch_sweep_lim<AXIS, HLLD_LIM_MP7>(solver, sp, st); break;
+    }
+}
+
+static void launch_ghost_cc(const Grid &G, double *const *arrs, int narr, cudaStream_t st) {
+    GhostParams gp = {};
+    for (int k = 0; k < narr; ++k) gp.v[k] = arrs[k];
+    gp.n0 = G.nxt;
+    gp.n1 = G.nyt;
+    gp.a0 = G.ng;
+    gp.b0 = G.ng + G.nx;
+    gp.a1 = G.ng;
+    gp.b1 = G.ng + G.ny;
+    gp.n_ph0 = G.nx;
+    gp.n_ph1 = G.ny;
+    gp.ng = G.ng;
+    gp.kind0 = G.bc_x;
+    gp.kind1 = G.bc_y;
+    int64_t cnt = (int64_t)gp.n0 * gp.n1 - (int64_t)(gp.b0 - gp.a0) * (gp.b1 - gp.a1);
+    ghost_kernel<<<dim3(grid1d(cnt), narr), kThreads, 0, st>>>(gp);
+}
+
+static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStream_t st) {
+    // Bxf: face rule along x, cell rule along y (grid.py:250-251)
+    GhostParams gp = {};
+    gp.v[0] = Bxf;
+    gp.n0 = G.nxt + 1;
+    gp.n1 = G.nyt;
+    gp.a0 = G.ng;
+    gp.b0 = G.ng + G.nx + (G.bc_x == HLLD_BC_OUTFLOW ? 1 : 0);
+    gp.a1 = G.ng;
+    gp.b1 = G.ng + G.ny;
+    gp.n_ph0 = G.nx;
+    gp.n_ph1 = G.ny;
+    gp.ng = G.ng;
+    gp.kind0 = G.bc_x;
+    gp.kind1 = G.bc_y;
+    gp.face0 = 1;
+    gp.face1 = 0;
+    int64_t cnt = (int64_t)gp.n0 * gp.n1 - (int64_t)(gp.b0 - gp.a0) * (gp.b1 - gp.a1);
+    ghost_kernel<<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gp);
+    // Byf: cell rule along x, face rule along y (grid.py:253-254)
+    GhostParams gq = {};
+    gq.v[0] = Byf;
+    gq.n0 = G.nxt;
+    gq.n1 = G.nyt + 1;
+    gq.a0 = G.ng;
+    gq.b0 = G.ng + G.nx;
+    gq.a1 = G.ng;
+    gq.b1 = G.ng + G.ny + (G.bc_y == HLLD_BC_OUTFLOW ? 1 : 0);
+    gq.n_ph0 = G.nx;
+    gq.n_ph1 = G.ny;
+    gq.ng = G.ng;
+    gq.kind0 = G.bc_x;
+    gq.kind1 = G.bc_y;
+    gq.face0 = 0;
+    gq.face1 = 1;
+    cnt = (int64_t)gq.n0 * gq.n1 - (int64_t)(gq.b0 - gq.a0) * (gq.b1 - gq.a1);
+    ghost_kernel<<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gq);
+}
+
+void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
+                       hlld_step_diag_t *diag, cudaStream_t st) {
+    Grid G = make_grid(g);
+    double *cons[6];
+    for (int k = 0; k < 6; ++k) cons[k] = (double *)s->cons[k];
+    double *prims[9];
+    for (int k = 0; k < 9; ++k) prims[k] = (double *)s->prims[k];
+    launch_ghost_faces(G, (double *)s->Bxf, (double *)s->Byf, st);
+    launch_ghost_cc(G, cons, 6, st);
+    C2PCellsParams cp = {};
+    cp.g = G;
+    for (int k = 0; k < 6; ++k) cp.U[k] = cons[k];
+    cp.Bxf = (const double *)s->Bxf;
+    cp.Byf = (const double *)s->Byf;
+    for (int k = 0; k < 9; ++k) cp.P[k] = prims[k];
+    cp.status = status;
+    cp.diag = diag;
+    c2p_cells_kernel<<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(cp);
+    launch_ghost_cc(G, prims, 9, st);
+}
+
+void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis,
+                    double *const *F, hlld_flux_diag_t *fdiag, cudaStream_t st) {
+    SweepParams sp = {};
+    sp.g = make_grid(g);
+    sp.rho = (const double *)s->prims[P_RHO];
+    sp.p = (const double *)s->prims[P_P];
+    sp.vx = (const double *)s->prims[P_VX];
+    sp.vy = (const double *)s->prims[P_VY];
+    sp.vz = (const double *)s->prims[P_VZ];
+    sp.bz = (const double *)s->prims[P_BZ];
+    sp.Bxf = (const double *)s->Bxf;
+    sp.Byf = (const double *)s->Byf;
+    for (int k = 0; k < NFLUX; ++k) sp.F[k] = F[k];
+    sp.diag = fdiag;
+    if (axis == 0) launch_sweep<0>(g->limiter, g->solver, sp, st);
+    else launch_sweep<1>(g->limiter, g->solver, sp, st);
+}
+
+// driver2d.py:104-105
+static const double kRK3[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
+static const double kRK2[2][3] = {{1.0, 0.0, 1.0}, {0.5, 0.5, 0.5}};
+
+void launch_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,
+                        const hlld_step_diag_t *diag, int stage, int scheme, double dt_host,
+                        const double *dt_dev, cudaStream_t st) {
+    Grid G = make_grid(g);
+    const double *w = scheme == 3 ? kRK3[stage] : kRK2[stage];
+    const int64_t ncorner = (int64_t)(G.nxt + 1) * (G.nyt + 1);
+    CtParams cp = {};
+    cp.g = G;
+    cp.vx = (const double *)s->prims[P_VX];
+    cp.vy = (const double *)s->prims[P_VY];
+    cp.Bxf = (const double *)s->Bxf;
+    cp.Byf = (const double *)s->Byf;
+    cp.FxD = sc.Fx[F_D];
+    cp.FyD = sc.Fy[F_D];
+    cp.FxBt = sc.Fx[F_BT];
+    cp.FyBt = sc.Fy[F_BT];
+    cp.diag = diag;
+    cp.upwind = g->upwind;
+    cp.Ez = sc.Ez;
+    ct_emf_kernel<<<grid1d(ncorner), kThreads, 0, st>>>(cp);
+    UpdateParams up = {};
+    up.g = G;
+    for (int k = 0; k < 6; ++k) {
+        up.U[k] = (double *)s->cons[k];
+        up.U0[k] = sc.U0[k];
+        up.Fx[k] = sc.Fx[k];
+        up.Fy[k] = sc.Fy[k];
+    }
+    up.Bxf = (double *)s->Bxf;
+    up.Byf = (double *)s->Byf;
+    up.Bx0 = sc.Bx0;
+    up.By0 = sc.By0;
+    up.Ez = sc.Ez;
+    up.dt_dev = dt_dev;
+    up.dt_host = dt_host;
+    up.a = w[0];
+    up.b = w[1];
+    up.c = w[2];
+    up.first_stage = stage == 0;
+    ct_update_kernel<<<grid1d((int64_t)(G.nx + 1) * (G.ny + 1)), kThreads, 0, st>>>(up);
+}
+
+void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,
+                       double dt_host, const double *dt_dev, int scheme, hlld_step_diag_t *diag,
+                       cudaStream_t st) {
+    const int nst = scheme == 3 ? 3 : 2;
+    for (int stage = 0; stage < nst; ++stage) {
+        // sweep counters and max |F_D| restart every stage; the CT scale is
+        // the current stage's (ct.py:114)
+        cudaMemsetAsync(diag, 0, sizeof(hlld_step_diag_t), st);
+        launch_sweep2d(g, s, 0, sc.Fx, &diag->sweep[0], st);
+        launch_sweep2d(g, s, 1, sc.Fy, &diag->sweep[1], st);
+        launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
+        launch_sync_state(g, s, nullptr, diag, st);
+    }
+}
+
+void launch_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,
+                          double *dt_dev, unsigned long long *work, cudaStream_t st) {
+    Grid G = make_grid(g);
+    cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), st);
+    SpeedParams sp = {};
+    sp.g = G;
+    for (int k = 0; k < 9; ++k) sp.P[k] = (const double *)s->prims[k];
+    sp.out = work;
+    speed_kernel<<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(sp);
+    dt_kernel<<<1, 1, 0, st>>>(work, g->dx, g->dy, cfl, dt_dev);
+}
+
+}  // namespace HLLD_NS
+}  // namespace hlld

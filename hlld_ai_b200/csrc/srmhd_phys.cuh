@@ -1,0 +1,885 @@
+// Device-side SRMHD physics for sm_100a: ideal-gas EOS, primitive <->
+// conserved maps, physical fluxes and wave speeds, HLLE, HLLD with its
+// total-pressure root solve, and Kastaun C2P.
+//
+// Every function is a per-element restatement of kemi2805/HLLD-AI's
+// element-wise PyTorch code (file:line cited at each function).  Operations
+// are written in the reference's order so that a translation unit built
+// with -fmad=false reproduces the reference arithmetic one rounding per
+// operation; built with FMA contraction the same source is the fast form.
+//
+// The real type of the reconstruction / flux algebra is a template
+// parameter (double, or float for the mixed-precision form); the Kastaun
+// C2P and the HLLD p* iteration take their own real type.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace hlld {
+
+enum { P_RHO = 0, P_VX, P_VY, P_VZ, P_P, P_EPS, P_BX, P_BY, P_BZ, NPRIM };
+enum { C_D = 0, C_SX, C_SY, C_SZ, C_TAU, C_BX, C_BY, C_BZ, NCONS };
+
+// C2P status bits (c2p.py:290-294, :360-362)
+constexpr uint8_t ST_BRACKET_OK = 1, ST_CONVERGED = 2, ST_V_CLAMPED = 4, ST_ATMO = 8,
+                  ST_BISECTED = 16;
+// Riemann flags (hlld.py:1487-1513)
+constexpr uint8_t RF_WAVE_ORDER_BAD = 1, RF_BN_ZERO = 2, RF_FAILED = 4;
+
+// Per-precision constants.  The FP64 values are the reference's own
+// (hlld.py:29, :1080, c2p.py:29, :318-319); FP32 keeps each one representable.
+template <typename T> struct K;
+template <> struct K<double> {
+    static constexpr double tiny = 1e-300;
+    static constexpr double c2p_tol = 1e-15;
+    static constexpr double pstar_tol = 1.0e-10;
+    static constexpr double weno_eps = 1e-40;
+    static constexpr double mp_eps = 1e-40;
+    static constexpr double safe_df = 1e-30;
+    static constexpr int mu_plus_iters = 50;
+};
+template <> struct K<float> {
+    static constexpr float tiny = 1e-30f;
+    static constexpr float c2p_tol = 1e-6f;
+    static constexpr float pstar_tol = 1e-5f;
+    static constexpr float weno_eps = 1e-30f;
+    static constexpr float mp_eps = 1e-30f;
+    static constexpr float safe_df = 1e-30f;
+    static constexpr int mu_plus_iters = 24;
+};
+
+// ── element-wise helpers with torch's semantics ─────────────────────────
+
+// torch.maximum / torch.minimum: NaN-propagating, ties keep the first operand
+template <typename T> __device__ __forceinline__ T tmax(T a, T b) {
+    if (isnan(a)) return a;
+    if (isnan(b)) return b;
+    return (a < b) ? b : a;
+}
+template <typename T> __device__ __forceinline__ T tmin(T a, T b) {
+    if (isnan(a)) return a;
+    if (isnan(b)) return b;
+    return (b < a) ? b : a;
+}
+template <typename T> __device__ __forceinline__ T clamp_lo(T x, T lo) { return (x < lo) ? lo : x; }
+template <typename T> __device__ __forceinline__ T clamp_hi(T x, T hi) { return (x > hi) ? hi : x; }
+// torch.sign: sign(NaN) = 0
+template <typename T> __device__ __forceinline__ T tsign(T x) {
+    return (x > T(0)) ? T(1) : ((x < T(0)) ? T(-1) : T(0));
+}
+// hlld.py:45-54 / c2p.py:32-36 _sdiv
+template <typename T> __device__ __forceinline__ T sdiv(T num, T den) {
+    if (fabs(den) < K<T>::tiny) {
+        T s = tsign(den);
+        if (s == T(0)) s = T(1);
+        return num / (s * K<T>::tiny);
+    }
+    return num / den;
+}
+
+// ── EOS: hybrid_eos(K=0, gamma, gamma_th=gamma) (eos.py:32-76) ───────────
+
+template <typename T> __device__ __forceinline__ T eos_press(T eps, T rho, T gamma) {
+    T e = tmax(eps, T(0));
+    return T(0) + (e - T(0)) * rho * (gamma - T(1));
+}
+template <typename T> __device__ __forceinline__ T eos_eps(T press, T rho, T gamma) {
+    return T(0) + (press - T(0)) / (rho * (gamma - T(1)));
+}
+template <typename T>
+__device__ __forceinline__ void eos_press_cs2(T eps, T rho, T gamma, T &p, T &cs2) {
+    T press = eos_press(eps, rho, gamma);
+    T h = T(1) + eps + press / rho;
+    T press_th = press - T(0);
+    p = press;
+    cs2 = (gamma * T(0) + gamma * press_th) / (rho * h);
+}
+
+// ── primitive -> conserved (hlld.py:185-217) ─────────────────────────────
+template <typename T> __device__ __forceinline__ void prim_to_cons(const T *P, T *C) {
+    T rho = P[P_RHO], vx = P[P_VX], vy = P[P_VY], vz = P[P_VZ];
+    T p = P[P_P], eps = P[P_EPS];
+    T Bx = P[P_BX], By = P[P_BY], Bz = P[P_BZ];
+    T v2 = vx * vx + vy * vy + vz * vz;
+    T W = T(1) / sqrt(clamp_lo(T(1) - v2, T(1e-10)));
+    T vB = vx * Bx + vy * By + vz * Bz;
+    T B2 = Bx * Bx + By * By + Bz * Bz;
+    T h = T(1) + eps + p / rho;
+    T rHW2 = rho * h * (W * W);
+    T D = rho * W;
+    C[C_D] = D;
+    C[C_SX] = (rHW2 + B2) * vx - vB * Bx;
+    C[C_SY] = (rHW2 + B2) * vy - vB * By;
+    C[C_SZ] = (rHW2 + B2) * vz - vB * Bz;
+    C[C_TAU] = rHW2 - p - D + T(0.5) * (B2 + B2 * v2 - vB * vB);
+    C[C_BX] = Bx;
+    C[C_BY] = By;
+    C[C_BZ] = Bz;
+}
+
+// ── Kastaun C2P (c2p.py:41-363) ──────────────────────────────────────────
+
+template <typename T> struct Kastaun {
+    T D, q, r[3], rNorm2, Bt[3], BtNorm2, B_dot_r, B2_rPerp2, v02, gamma;
+
+    // c2p.py:48-106
+    __device__ __forceinline__ void init(const T *C, T g) {
+        T Dv = C[C_D];
+        T Sx = C[C_SX], Sy = C[C_SY], Sz = C[C_SZ];
+        T tau = C[C_TAU];
+        T Bx = C[C_BX], By = C[C_BY], Bz = C[C_BZ];
+        tau = clamp_lo(tau, T(0));
+        T S2 = Sx * Sx + Sy * Sy + Sz * Sz;
+        T Snorm = sqrt(S2);
+        T S_max = Dv + tau;
+        bool too_large = Snorm > S_max;
+        T fac = too_large ? T(0.9999) * S_max / (Snorm + K<T>::tiny) : T(1);
+        Sx = Sx * fac;
+        Sy = Sy * fac;
+        Sz = Sz * fac;
+        S2 = Sx * Sx + Sy * Sy + Sz * Sz;
+        T B2 = Bx * Bx + By * By + Bz * Bz;
+        T BdotS = Bx * Sx + By * Sy + Bz * Sz;
+        D = Dv;
+        q = tau / (Dv + K<T>::tiny);
+        r[0] = Sx / (Dv + K<T>::tiny);
+        r[1] = Sy / (Dv + K<T>::tiny);
+        r[2] = Sz / (Dv + K<T>::tiny);
+        rNorm2 = S2 / (Dv * Dv + K<T>::tiny);
+        T sqrtD = sqrt(Dv + K<T>::tiny);
+        Bt[0] = Bx / sqrtD;
+        Bt[1] = By / sqrtD;
+        Bt[2] = Bz / sqrtD;
+        BtNorm2 = B2 / (Dv + K<T>::tiny);
+        B_dot_r = BdotS / (Dv * sqrtD + K<T>::tiny);
+        B2_rPerp2 = rNorm2 * BtNorm2 - B_dot_r * B_dot_r;
+        v02 = rNorm2 / (rNorm2 + T(1));
+        gamma = g;
+    }
+    // c2p.py:110-127
+    __device__ __forceinline__ T chi(T mu) const { return T(1) / (T(1) + mu * BtNorm2); }
+    __device__ __forceinline__ T rbar2(T mu) const {
+        T c = chi(mu);
+        return rNorm2 * (c * c) + mu * c * (T(1) + c) * (B_dot_r * B_dot_r);
+    }
+    __device__ __forceinline__ T qbar(T mu) const {
+        T c = chi(mu);
+        T mc = mu * c;
+        return q - T(0.5) * BtNorm2 - T(0.5) * (mc * mc) * B2_rPerp2;
+    }
+    __device__ __forceinline__ T fa(T mu) const { return mu * sqrt(T(1) + rbar2(mu)) - T(1); }
+
+    // c2p.py:129-158 (f only, or the full set for _finish)
+    __device__ __forceinline__ T master(T mu, T *rho_o = nullptr, T *eps_o = nullptr) const {
+        T qb = qbar(mu);
+        T rb2 = rbar2(mu);
+        T vhat2 = tmin((mu * mu) * rb2, v02);
+        T What = T(1) / sqrt(clamp_lo(T(1) - vhat2, T(1e-10)));
+        T rhohat0 = D / What;
+        T rhohat = tmin(tmax(rhohat0, T(1e-12)), T(1e15));
+        T epshat0 = What * (qb - mu * rb2) + vhat2 * (What * What) / (T(1) + What);
+        T epshat = tmin(tmax(epshat0, T(0)), T(1e5));
+        T phat = eos_press(epshat, rhohat, gamma);
+        T ahat = phat / (rhohat * (T(1) + epshat) + K<T>::tiny);
+        T h_eff = (T(1) + ahat) * (T(1) + epshat);
+        T nu_A = h_eff / What;
+        T nu_B = (T(1) + ahat) * (T(1) + qb - mu * rb2);
+        T nu = tmax(nu_A, nu_B);
+        if (rho_o) *rho_o = rhohat;
+        if (eps_o) *eps_o = epshat;
+        return mu - sdiv(T(1), nu + mu * rb2);
+    }
+
+    // c2p.py:162-184: bisection of f_a on [0, 1] (its bracket width is
+    // exactly 2^-k after k halvings, so the batch early stop never fires
+    // early).  f_a(mu_lo) is a deterministic function of mu_lo, so the value
+    // from the previous iteration is reused instead of re-evaluated.
+    __device__ __forceinline__ T mu_plus() const {
+        T lo = T(0), hi = T(1) / (T(1) + K<T>::tiny);
+        T f_lo = fa(lo);
+#pragma unroll 1
+        for (int it = 0; it < K<T>::mu_plus_iters; ++it) {
+            T mid = T(0.5) * (lo + hi);
+            T f_mid = fa(mid);
+            bool lft = (f_lo * f_mid) <= T(0);
+            if (lft) {
+                hi = mid;
+            } else {
+                lo = mid;
+                f_lo = f_mid;
+            }
+        }
+        return hi;
+    }
+};
+
+template <typename T> struct C2POut {
+    T rho, v[3], p, eps;
+    uint8_t status;
+};
+
+// c2p.py:268-310 _finish
+template <typename T>
+__device__ __forceinline__ void kastaun_finish(const Kastaun<T> &k, T mu, bool converged,
+                                               bool good_bracket, C2POut<T> &o) {
+    T rho, eps;
+    k.master(mu, &rho, &eps);
+    T c = k.chi(mu);
+    T mc = mu * c;
+    T mB = mu * k.B_dot_r;
+    T v[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = mc * (k.r[i] + mB * k.Bt[i]);
+    T v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    T lim = T(1) - T(1e-10);
+    T v2c = clamp_hi(v2, lim);
+    T norm = (v2 > lim) ? sqrt(v2c / (v2 + K<T>::tiny)) : T(1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) o.v[i] = v[i] * norm;
+    o.rho = rho;
+    o.eps = eps;
+    o.p = eos_press(eps, rho, k.gamma);
+    uint8_t st = 0;
+    if (good_bracket) st |= ST_BRACKET_OK;
+    if (converged) st |= ST_CONVERGED;
+    if (v2 > lim) st |= ST_V_CLAMPED;
+    o.status = st;
+}
+
+// c2p.py:188-236 invert, stopping per element
+template <typename T>
+__device__ __forceinline__ void kastaun_invert(const Kastaun<T> &k, T mu_plus, C2POut<T> &o) {
+    const T tol = K<T>::c2p_tol;
+    T mu_lo = T(0);
+    T mu_hi = mu_plus * (T(1) - T(1e-10));
+    T f_lo = k.master(mu_lo);
+    T f_hi = k.master(mu_hi);
+    bool good_bracket = (f_lo * f_hi) < T(0);
+    T x0 = mu_lo, x1 = mu_hi, f0 = f_lo, f1 = f_hi;
+#pragma unroll 1
+    for (int it = 0; it < 60; ++it) {
+        if (fabs(f1) < tol) break;
+        T df = f1 - f0;
+        bool safe = fabs(df) > T(1e-30);
+        T x2s = safe ? x1 - f1 * (x1 - x0) / df : T(0.5) * (x0 + x1);
+        bool inb = (x2s - x0) * (x2s - x1) < T(0);
+        T x2 = inb ? x2s : T(0.5) * (x0 + x1);
+        T f2 = k.master(x2);
+        bool lft = (f0 * f2) <= T(0);
+        if (!lft) {
+            x0 = x1;
+            f0 = f1;
+        }
+        x1 = x2;
+        f1 = f2;
+    }
+    kastaun_finish(k, x1, fabs(f1) < tol, good_bracket, o);
+}
+
+// c2p.py:238-266 invert_bisection.  A bracket collapsed onto adjacent
+// doubles maps onto itself, so stopping at the first unchanged iteration
+// returns the 200-step answer.
+template <typename T>
+__device__ __forceinline__ void kastaun_bisect(const Kastaun<T> &k, T mu_plus, C2POut<T> &o) {
+    const T tol = K<T>::c2p_tol;
+    T x0 = T(0);
+    T x1 = mu_plus * (T(1) - T(1e-10));
+    T f0 = k.master(x0);
+    T f1 = k.master(x1);
+    bool good_bracket = (f0 * f1) < T(0);
+#pragma unroll 1
+    for (int it = 0; it < 200; ++it) {
+        T xm = T(0.5) * (x0 + x1);
+        T fm = k.master(xm);
+        bool left = (f0 * fm) <= T(0);
+        T nx0 = left ? x0 : xm, nf0 = left ? f0 : fm;
+        T nx1 = left ? xm : x1, nf1 = left ? fm : f1;
+        bool same = (nx0 == x0) && (nx1 == x1) && (nf0 == f0) && (nf1 == f1);
+        x0 = nx0;
+        f0 = nf0;
+        x1 = nx1;
+        f1 = nf1;
+        if (same) break;
+    }
+    bool pick = fabs(f0) < fabs(f1);
+    T mu = pick ? x0 : x1;
+    T fmu = pick ? f0 : f1;
+    kastaun_finish(k, mu, fabs(fmu) < tol, good_bracket, o);
+}
+
+// c2p.py:313-363 conservative_to_primitive for one element; P gets the nine
+// primitives (B copied from C).
+template <typename T>
+__device__ __forceinline__ uint8_t cons_to_prim(const T *C, T gamma, T atmo_rho, T atmo_eps,
+                                                T *P) {
+    Kastaun<T> k;
+    k.init(C, gamma);
+    T mp = k.mu_plus();
+    C2POut<T> o;
+    kastaun_invert(k, mp, o);
+    uint8_t extra = 0;
+    if (!(o.status & ST_CONVERGED) && (o.status & ST_BRACKET_OK)) {
+        kastaun_bisect(k, mp, o);
+        o.status |= ST_BRACKET_OK;
+        extra = ST_BISECTED;
+    }
+    T rho = o.rho, eps = o.eps, vx = o.v[0], vy = o.v[1], vz = o.v[2];
+    bool atmo = rho < atmo_rho;
+    if (atmo) {
+        rho = atmo_rho;
+        eps = atmo_eps;
+        vx = T(0);
+        vy = T(0);
+        vz = T(0);
+    }
+    P[P_RHO] = rho;
+    P[P_VX] = vx;
+    P[P_VY] = vy;
+    P[P_VZ] = vz;
+    P[P_P] = eos_press(eps, rho, gamma);
+    P[P_EPS] = eps;
+    P[P_BX] = C[C_BX];
+    P[P_BY] = C[C_BY];
+    P[P_BZ] = C[C_BZ];
+    return (uint8_t)(o.status | extra | (atmo ? ST_ATMO : 0));
+}
+
+// ── physical fluxes (hlld.py:57-113, :223-334) ───────────────────────────
+
+template <typename T> struct Side {
+    T u[NCONS], f[NCONS];
+};
+
+// hlld.py:100-113 compute_cp_cm (flat space)
+template <typename T>
+__device__ __forceinline__ void cp_cm(T v02, T u0, T vd, T &cp, T &cm) {
+    T u0_sq = u0 * u0;
+    T a = u0_sq * (T(1) - v02) + v02 * T(1);
+    T b = T(2) * (T(0) * T(1) * v02 - u0_sq * vd * (T(1) - v02));
+    T c = u0_sq * (vd * vd) * (T(1) - v02) - v02 * (T(1) - T(0) * T(0) * T(1));
+    T det = sqrt(clamp_lo(b * b - T(4) * a * c, T(0)));
+    T a_safe = clamp_lo(a, K<T>::tiny);
+    T c1 = T(0.5) * (det - b) / a_safe;
+    T c2 = T(-0.5) * (det + b) / a_safe;
+    cp = tmax(c1, c2);
+    cm = tmin(c1, c2);
+}
+
+// hlld.py:57-62
+template <typename T> __device__ __forceinline__ T lorentz_W(const T *P) {
+    T v2 = P[P_VX] * P[P_VX] + P[P_VY] * P[P_VY] + P[P_VZ] * P[P_VZ];
+    T v2s = clamp_hi(v2, T(1) - T(1e-10));
+    return T(1) / sqrt(T(1) - v2s);
+}
+// hlld.py:84-90
+template <typename T> __device__ __forceinline__ T comp_b2(const T *P, T W) {
+    T B2 = P[P_BX] * P[P_BX] + P[P_BY] * P[P_BY] + P[P_BZ] * P[P_BZ];
+    T vdotB = P[P_VX] * P[P_BX] + P[P_VY] * P[P_BY] + P[P_VZ] * P[P_BZ];
+    return B2 / (W * W) + vdotB * vdotB;
+}
+
+// one side of compute_srmhd_fluxes (hlld.py:234-332)
+template <int IDIR, typename T>
+__device__ __forceinline__ void phys_side(const T *P, T gamma, Side<T> &s, T &cp, T &cm) {
+    T W = lorentz_W(P);
+    T p, cs2;
+    eos_press_cs2(P[P_EPS], P[P_RHO], gamma, p, cs2);
+    T b2 = comp_b2(P, W);
+    T v[3] = {P[P_VX], P[P_VY], P[P_VZ]};
+    T B[3] = {P[P_BX], P[P_BY], P[P_BZ]};
+    T vdotB = v[0] * B[0] + v[1] * B[1] + v[2] * B[2];
+    T bt = W * vdotB;
+    T bs[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) bs[i] = B[i] / W + vdotB * v[i] * W;
+    T rho = P[P_RHO], eps = P[P_EPS];
+    T h = T(1) + eps + p / rho;
+    T v02 = cs2 + (b2 / (rho * h + b2)) * (T(1) - cs2);
+    cp_cm(v02, W, v[IDIR], cp, cm);
+    T d = rho * W;
+    T rhb2 = rho * h + b2;
+    T Pb2 = p + T(0.5) * b2;
+    T vd = v[IDIR];
+    T bdir = bs[IDIR];
+    s.u[C_D] = d;
+    s.f[C_D] = d * vd;
+    T Tt = rhb2 * (W * W) + Pb2 * T(-1) - bt * bt;
+    s.u[C_TAU] = Tt - d;
+    s.f[C_TAU] = (rhb2 * (W * W) * vd - bt * bdir) - d * vd;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        T delta = (i == IDIR) ? T(1) : T(0);
+        T uDi = W * v[i];
+        s.u[C_SX + i] = rhb2 * W * uDi - bt * bs[i];
+        s.f[C_SX + i] = rhb2 * (W * vd) * uDi + Pb2 * delta - bdir * bs[i];
+    }
+    T Bdir = B[IDIR];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        s.u[C_BX + i] = B[i];
+        s.f[C_BX + i] = vd * B[i] - v[i] * Bdir;
+    }
+}
+
+template <typename T> struct Phys {
+    Side<T> L, R;
+    T cmax, cmin;
+};
+
+template <int IDIR, typename T>
+__device__ __forceinline__ void srmhd_fluxes(const T *PL, const T *PR, T gamma, Phys<T> &ph) {
+    T cp_l, cm_l, cp_r, cm_r;
+    phys_side<IDIR>(PL, gamma, ph.L, cp_l, cm_l);
+    phys_side<IDIR>(PR, gamma, ph.R, cp_r, cm_r);
+    T cmax = clamp_lo(tmax(cp_l, cp_r), T(0));
+    T cmin = clamp_lo(tmax(-cm_l, -cm_r), T(0));
+    bool both_small = (cmax < T(1e-12)) && (cmin < T(1e-12));
+    if (both_small) {
+        cmax = T(1);
+        cmin = T(1);
+    }
+    ph.cmax = cmax;
+    ph.cmin = cmin;
+}
+
+// hlld.py:161-168
+template <typename T> __device__ __forceinline__ T hf(T fL, T fR, T uL, T uR, T cm, T cx) {
+    return (cx * fL + cm * fR - cx * cm * (uR - uL)) / (cx + cm);
+}
+template <typename T> __device__ __forceinline__ T hu(T fL, T fR, T uL, T uR, T cm, T cx) {
+    return (cx * uR + cm * uL + fL - fR) / (cx + cm);
+}
+
+// Per-face solver output.  F has the eight conserved-variable fluxes; U the
+// resolved state (only filled when want_u).
+template <typename T> struct FaceOut {
+    T F[NCONS];
+    T U[NCONS];
+    T pstar;
+    int32_t err, iters;
+    uint8_t flags;
+};
+
+// hlld.py:1036-1042
+template <typename T>
+__device__ __forceinline__ T hlle_p_estimate(const T *PL, const T *PR, T gamma) {
+    T pl, pr, c;
+    eos_press_cs2(PL[P_EPS], PL[P_RHO], gamma, pl, c);
+    eos_press_cs2(PR[P_EPS], PR[P_RHO], gamma, pr, c);
+    T wl = lorentz_W(PL), wr = lorentz_W(PR);
+    T b2l = comp_b2(PL, wl), b2r = comp_b2(PR, wr);
+    return clamp_lo(T(0.5) * (pl + T(0.5) * b2l + pr + T(0.5) * b2r), T(1e-30));
+}
+
+// hlld.py:1005-1044 hlle_flux
+template <int IDIR, typename T>
+__device__ __forceinline__ void hlle_face(const T *PL, const T *PR, T gamma, bool want_u,
+                                          bool want_pstar, FaceOut<T> &o) {
+    Phys<T> ph;
+    srmhd_fluxes<IDIR>(PL, PR, gamma, ph);
+    T cm = ph.cmin, cx = ph.cmax;
+#pragma unroll
+    for (int k = 0; k < NCONS; ++k) {
+        T fL = ph.L.f[k], fR = ph.R.f[k], uL = ph.L.u[k], uR = ph.R.u[k];
+        T fH = hf(fL, fR, uL, uR, cm, cx);
+        o.F[k] = (cx <= T(0)) ? fR : ((cm <= T(0)) ? fL : fH);
+        if (want_u) {
+            T uH = hu(fL, fR, uL, uR, cm, cx);
+            o.U[k] = (cm <= T(0)) ? uL : ((cx <= T(0)) ? uR : uH);
+        }
+    }
+    o.pstar = want_pstar ? hlle_p_estimate(PL, PR, gamma) : T(0);
+    o.err = 0;
+    o.iters = 0;
+    o.flags = 0;
+}
+
+// ── HLLD (hlld.py:366-605, :669-746, :1202-1543) ─────────────────────────
+
+// HLLDComputation R vectors (hlld.py:401-428), energy form
+template <typename T> struct HlldR {
+    T RSiL, RSiR, RS1L, RS1R, RS2L, RS2R;
+    T RBiL, RBiR, RB1L, RB1R, RB2L, RB2R;
+    T RTL, RTR, RDL, RDR;
+    T S_L, S_R, BnL, BnR, cm, cx;
+};
+
+template <typename T> struct HlldV {
+    T vaL, vaR, vt1aL, vt2aL, vt1aR, vt2aR;
+    T Bt1aL, Bt2aL, Bt1aR, Bt2aR;
+    T sqL, sqR, DaL, DaR, TauaL, TauaR;
+    T SaL, SaR, St1aL, St2aL, St1aR, St2aR;
+    T laL, laR, Kt1aL, Kt2aL, Kt1aR, Kt2aR;
+    T Bt1c, Bt2c, KaL2, KaR2, KaLBc, KaRBc;
+};
+
+// hlld.py:431-583 compute_all_variables.  FULL = false computes only what
+// the residual needs.
+template <bool FULL, typename T>
+__device__ __forceinline__ void hlld_vars(const HlldR<T> &c, T p, HlldV<T> &o) {
+    const T cm = c.cm, cx = c.cx, ncm = -c.cm;
+    const T RSiL = c.RSiL, RSiR = c.RSiR, RS1L = c.RS1L, RS1R = c.RS1R;
+    const T RS2L = c.RS2L, RS2R = c.RS2R;
+    const T RB1L = c.RB1L, RB1R = c.RB1R, RB2L = c.RB2L, RB2R = c.RB2R;
+    const T RTL = c.RTL, RTR = c.RTR, BnL = c.BnL, BnR = c.BnR;
+
+    T AL = RSiL - ncm * RTL + p * (T(1) - cm * cm);
+    T AR = RSiR - cx * RTR + p * (T(1) - cx * cx);
+    T GL = RB1L * RB1L + RB2L * RB2L;
+    T GR = RB1R * RB1R + RB2R * RB2R;
+    T CL = RS1L * RB1L + RS2L * RB2L;
+    T CR = RS1R * RB1R + RS2R * RB2R;
+    T QL = -AL - GL + (BnL * BnL) * (T(1) - cm * cm);
+    T QR = -AR - GR + (BnR * BnR) * (T(1) - cx * cx);
+    T XL = BnL * (AL * ncm * BnL + CL) - (AL + GL) * (ncm * p + RTL);
+    T XR = BnR * (AR * cx * BnR + CR) - (AR + GR) * (cx * p + RTR);
+
+    T vaL = sdiv(BnL * (AL * BnL + ncm * CL) - (AL + GL) * (p + RSiL), XL);
+    T vaR = sdiv(BnR * (AR * BnR + cx * CR) - (AR + GR) * (p + RSiR), XR);
+    T vt1aL = sdiv(QL * RS1L + RB1L * (CL + BnL * (ncm * RSiL - RTL)), XL);
+    T vt1aR = sdiv(QR * RS1R + RB1R * (CR + BnR * (cx * RSiR - RTR)), XR);
+    T vt2aL = sdiv(QL * RS2L + RB2L * (CL + BnL * (ncm * RSiL - RTL)), XL);
+    T vt2aR = sdiv(QR * RS2R + RB2R * (CR + BnR * (cx * RSiR - RTR)), XR);
+
+    T Bt1aL = sdiv(RB1L - BnL * vt1aL, ncm - vaL);
+    T Bt1aR = sdiv(RB1R - BnR * vt1aR, cx - vaR);
+    T Bt2aL = sdiv(RB2L - BnL * vt2aL, ncm - vaL);
+    T Bt2aR = sdiv(RB2R - BnR * vt2aR, cx - vaR);
+
+    T vRS_AL = vaL * RSiL + vt1aL * RS1L + vt2aL * RS2L;
+    T vRS_AR = vaR * RSiR + vt1aR * RS1R + vt2aR * RS2R;
+
+    T waL = p + sdiv(RTL - vRS_AL, ncm - vaL);
+    T waR = p + sdiv(RTR - vRS_AR, cx - vaR);
+
+    T sqL = sqrt(clamp_lo(waL, T(0)));
+    T sqR = sqrt(clamp_lo(waR, T(0)));
+
+    const T S_L = c.S_L, S_R = c.S_R;
+    T dL = ncm * p + RTL - BnL * S_L * sqL;
+    T dR = cx * p + RTR + BnR * S_R * sqR;
+
+    T KaL = sdiv(RSiL + p - c.RBiL * S_L * sqL, dL);
+    T KaR = sdiv(RSiR + p + c.RBiR * S_R * sqR, dR);
+    T Kt1aL = sdiv(RS1L - RB1L * S_L * sqL, dL);
+    T Kt1aR = sdiv(RS1R + RB1R * S_R * sqR, dR);
+    T Kt2aL = sdiv(RS2L - RB2L * S_L * sqL, dL);
+    T Kt2aR = sdiv(RS2R + RB2R * S_R * sqR, dR);
+
+    T laL = KaL, laR = KaR;
+    T denom_ll = laR - laL;
+    T Bic = BnR;
+    T Bt1c = sdiv((Bt1aR * (laR - vaR) + BnR * vt1aR) - (Bt1aL * (laL - vaL) + BnL * vt1aL),
+                  denom_ll);
+    T Bt2c = sdiv((Bt2aR * (laR - vaR) + BnR * vt2aR) - (Bt2aL * (laL - vaL) + BnL * vt2aL),
+                  denom_ll);
+
+    o.sqL = sqL;
+    o.sqR = sqR;
+    o.laL = laL;
+    o.laR = laR;
+    o.KaL2 = KaL * KaL + Kt1aL * Kt1aL + Kt2aL * Kt2aL;
+    o.KaR2 = KaR * KaR + Kt1aR * Kt1aR + Kt2aR * Kt2aR;
+    o.KaLBc = KaL * Bic + Kt1aL * Bt1c + Kt2aL * Bt2c;
+    o.KaRBc = KaR * Bic + Kt1aR * Bt1c + Kt2aR * Bt2c;
+    if (FULL) {
+        T DaL = sdiv(c.RDL, ncm - vaL);
+        T DaR = sdiv(c.RDR, cx - vaR);
+        T vBaL = vaL * BnL + vt1aL * Bt1aL + vt2aL * Bt2aL;
+        T vBaR = vaR * BnR + vt1aR * Bt1aR + vt2aR * Bt2aR;
+        T TauaL = sdiv(RTL + p * vaL - vBaL * BnL, ncm - vaL) - DaL;
+        T TauaR = sdiv(RTR + p * vaR - vBaR * BnR, cx - vaR) - DaR;
+        o.SaL = (TauaL + DaL + p) * vaL - vBaL * BnL;
+        o.SaR = (TauaR + DaR + p) * vaR - vBaR * BnR;
+        o.St1aL = (TauaL + DaL + p) * vt1aL - vBaL * Bt1aL;
+        o.St1aR = (TauaR + DaR + p) * vt1aR - vBaR * Bt1aR;
+        o.St2aL = (TauaL + DaL + p) * vt2aL - vBaL * Bt2aL;
+        o.St2aR = (TauaR + DaR + p) * vt2aR - vBaR * Bt2aR;
+        o.DaL = DaL;
+        o.DaR = DaR;
+        o.TauaL = TauaL;
+        o.TauaR = TauaR;
+        o.vaL = vaL;
+        o.vaR = vaR;
+        o.vt1aL = vt1aL;
+        o.vt2aL = vt2aL;
+        o.vt1aR = vt1aR;
+        o.vt2aR = vt2aR;
+        o.Bt1aL = Bt1aL;
+        o.Bt2aL = Bt2aL;
+        o.Bt1aR = Bt1aR;
+        o.Bt2aR = Bt2aR;
+        o.Kt1aL = Kt1aL;
+        o.Kt2aL = Kt2aL;
+        o.Kt1aR = Kt1aR;
+        o.Kt2aR = Kt2aR;
+        o.Bt1c = Bt1c;
+        o.Bt2c = Bt2c;
+    }
+}
+
+// hlld.py:586-602 residual
+template <typename T> __device__ __forceinline__ T hlld_residual(const HlldR<T> &c, T p) {
+    HlldV<T> v;
+    hlld_vars<false>(c, p, v);
+    T denom_R = c.S_R * v.sqR - v.KaRBc;
+    T denom_L = c.S_L * v.sqL + v.KaLBc;
+    return (v.laL - v.laR) + c.BnL * (sdiv(T(1) - v.KaR2, denom_R) + sdiv(T(1) - v.KaL2, denom_L));
+}
+
+// hlld.py:1202-1543 hlld_flux for one face.  T is the algebra's real type,
+// TC the real type of the HLL-state C2P (legacy bracket) and TP that of the
+// p* iteration; the fast and exact forms use double for all three.
+template <int IDIR, typename T, typename TC = T, typename TP = T>
+__device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, bool want_u,
+                                          FaceOut<T> &o) {
+    constexpr int i = IDIR, t1 = (IDIR + 1) % 3, t2 = (IDIR + 2) % 3;
+    Phys<T> ph;
+    srmhd_fluxes<IDIR>(PL, PR, gamma, ph);
+    const T cm = ph.cmin, cx = ph.cmax;
+    T fH[NCONS], uH[NCONS];
+#pragma unroll
+    for (int k = 0; k < NCONS; ++k) {
+        fH[k] = hf(ph.L.f[k], ph.R.f[k], ph.L.u[k], ph.R.u[k], cm, cx);
+        uH[k] = hu(ph.L.f[k], ph.R.f[k], ph.L.u[k], ph.R.u[k], cm, cx);
+    }
+
+    // legacy bracket (hlld.py:1253-1263): total pressure of the HLL state
+    TP p_hll;
+    {
+        TC Ch[NCONS], Ph[NPRIM];
+#pragma unroll
+        for (int k = 0; k < NCONS; ++k) Ch[k] = (TC)uH[k];
+        cons_to_prim<TC>(Ch, (TC)gamma, TC(1e-10), TC(1e-10), Ph);
+        TC pp, cs2;
+        eos_press_cs2(Ph[P_EPS], Ph[P_RHO], (TC)gamma, pp, cs2);
+        TC w = lorentz_W(Ph);
+        TC b2 = comp_b2(Ph, w);
+        p_hll = (TP)(pp + TC(0.5) * b2);
+    }
+
+    // p0 from the Bn = 0 limit (hlld.py:1265-1287)
+    constexpr int Sn = C_SX + i, Bn = C_BX + i;
+    TP a = (TP)fH[C_TAU] + (TP)fH[C_D];
+    TP b = -(TP)fH[Sn] - (TP)uH[C_TAU] - (TP)uH[C_D];
+    TP cq = (TP)uH[Sn];
+    TP disc = b * b - TP(4) * a * cq;
+    disc = clamp_lo(disc, TP(0));
+    bool abig = fabs(a) > TP(1e-14);
+    TP safe_a = abig ? a : TP(1);
+    TP safe_b = abig ? b : TP(1);
+    TP v_star = abig ? (-b - sqrt(disc)) / (TP(2) * safe_a) : -cq / safe_b;
+    v_star = clamp_hi(clamp_lo(v_star, -(TP(1) - TP(1e-10))), TP(1) - TP(1e-10));
+    TP p0 = (TP)fH[Sn] - ((TP)fH[C_TAU] + (TP)fH[C_D]) * v_star;
+    p0 = clamp_lo(p0, TP(1e-30));
+
+    const T BnL = ph.L.u[Bn], BnR = ph.R.u[Bn];
+    TP Bn2 = TP(0.5) * ((TP)BnL * (TP)BnL + (TP)BnR * (TP)BnR);
+    bool use_p0 = (Bn2 / p_hll) < TP(0.1);
+    TP p_lo = use_p0 ? p0 * TP(0.99) : p_hll * TP(0.99);
+    TP p_hi = use_p0 ? p0 * TP(1.01) : p_hll * TP(1.01);
+    bool bn_zero = (fabs(BnL) < T(1e-14)) && (fabs(BnR) < T(1e-14));
+
+    // R vectors on the energy-form state (hlld.py:337-360, :401-428)
+    HlldR<TP> C;
+    {
+        const TP pcm = (TP)cm, pcx = (TP)cx;
+        TP UiL[NCONS], UiR[NCONS], FiL[NCONS], FiR[NCONS];
+#pragma unroll
+        for (int k = 0; k < NCONS; ++k) {
+            UiL[k] = (TP)ph.L.u[k];
+            UiR[k] = (TP)ph.R.u[k];
+            FiL[k] = (TP)ph.L.f[k];
+            FiR[k] = (TP)ph.R.f[k];
+        }
+        UiL[C_TAU] = (TP)(ph.L.u[C_TAU] + ph.L.u[C_D]);
+        UiR[C_TAU] = (TP)(ph.R.u[C_TAU] + ph.R.u[C_D]);
+        FiL[C_TAU] = (TP)(ph.L.f[C_TAU] + ph.L.f[C_D]);
+        FiR[C_TAU] = (TP)(ph.R.f[C_TAU] + ph.R.f[C_D]);
+        C.cm = pcm;
+        C.cx = pcx;
+        C.RSiL = -pcm * UiL[C_SX + i] - FiL[C_SX + i];
+        C.RSiR = pcx * UiR[C_SX + i] - FiR[C_SX + i];
+        C.RS1L = -pcm * UiL[C_SX + t1] - FiL[C_SX + t1];
+        C.RS1R = pcx * UiR[C_SX + t1] - FiR[C_SX + t1];
+        C.RS2L = -pcm * UiL[C_SX + t2] - FiL[C_SX + t2];
+        C.RS2R = pcx * UiR[C_SX + t2] - FiR[C_SX + t2];
+        C.RBiL = -pcm * UiL[C_BX + i] - FiL[C_BX + i];
+        C.RBiR = pcx * UiR[C_BX + i] - FiR[C_BX + i];
+        C.RB1L = -pcm * UiL[C_BX + t1] - FiL[C_BX + t1];
+        C.RB1R = pcx * UiR[C_BX + t1] - FiR[C_BX + t1];
+        C.RB2L = -pcm * UiL[C_BX + t2] - FiL[C_BX + t2];
+        C.RB2R = pcx * UiR[C_BX + t2] - FiR[C_BX + t2];
+        C.RTL = -pcm * UiL[C_TAU] - FiL[C_TAU];
+        C.RTR = pcx * UiR[C_TAU] - FiR[C_TAU];
+        C.RDL = -pcm * UiL[C_D] - FiL[C_D];
+        C.RDR = pcx * UiR[C_D] - FiR[C_D];
+        C.S_L = tsign(UiL[C_BX + i]);
+        C.S_R = tsign(UiR[C_BX + i]);
+        C.BnL = UiL[C_BX + i];
+        C.BnR = UiR[C_BX + i];
+    }
+
+    TP f_lo = hlld_residual(C, p_lo);
+    TP f_hi = hlld_residual(C, p_hi);
+    // bracket widening (hlld.py:1314-1321)
+#pragma unroll 1
+    for (int w = 0; w < 5; ++w) {
+        if (!((f_lo * f_hi) > TP(0))) break;
+        p_lo = p_lo / TP(2);
+        p_hi = p_hi * TP(2);
+        f_lo = hlld_residual(C, p_lo);
+        f_hi = hlld_residual(C, p_hi);
+    }
+
+    // clamped secant (hlld.py:669-746, _PSTAR_TOL hlld.py:1080, 30 iterations)
+    const TP tol = K<TP>::pstar_tol;
+    TP x0 = p_lo, x1 = p_hi, f0 = f_lo, f1 = f_hi;
+    int32_t err = 30, iters_used = 30;
+    bool done = false;
+#pragma unroll 1
+    for (int it = 1; it <= 30; ++it) {
+        if (fabs(f1) < tol) {
+            err = 0;
+            iters_used = it - 1;
+            done = true;
+            break;
+        }
+        TP df = f1 - f0;
+        bool safe = fabs(df) > TP(1e-30) * fabs(f1);
+        TP dx = safe ? f1 * (x1 - x0) / df : TP(0);
+        TP x2 = x1 - dx;
+        x2 = clamp_lo(x2, TP(1e-30));
+        TP f2 = hlld_residual(C, x2);
+        x0 = x1;
+        f0 = f1;
+        x1 = x2;
+        f1 = f2;
+    }
+    if (!done && fabs(f1) < tol) {
+        err = 0;
+        iters_used = 30;
+    }
+    TP p_star = x1;
+
+    HlldV<TP> V;
+    hlld_vars<true>(C, p_star, V);
+
+    // star states (hlld.py:1359-1445), in the algebra's real type
+    const TP pcm = (TP)cm, pcx = (TP)cx;
+    const TP laL = V.laL, laR = V.laR;
+    TP fac = sdiv(TP(1) - V.KaL2, -C.S_L * V.sqL - V.KaLBc);
+    TP vc = laL - (TP)BnR * fac;
+    TP vt1 = V.Kt1aL - V.Bt1c * fac;
+    TP vt2 = V.Kt2aL - V.Bt2c * fac;
+    TP vcomp[3], Bc[3];
+    vcomp[i] = vc;
+    vcomp[t1] = vt1;
+    vcomp[t2] = vt2;
+    Bc[i] = (TP)BnR;
+    Bc[t1] = V.Bt1c;
+    Bc[t2] = V.Bt2c;
+    TP vBc = vc * Bc[i] + vt1 * V.Bt1c + vt2 * V.Bt2c;
+
+    bool wave_order_bad = (V.vaR > pcx) || (V.vaL < -pcm) || (vc < laL) || (vc > laR);
+    bool failed = (err > 0) || wave_order_bad || bn_zero;
+
+    if (failed) {
+#pragma unroll
+        for (int k = 0; k < NCONS; ++k) {
+            o.F[k] = fH[k];
+            if (want_u) o.U[k] = uH[k];
+        }
+        o.pstar = (T)(-fabs(p_hll) - TP(1e-10));
+    } else {
+        TP uaL[NCONS], uaR[NCONS];
+        uaL[C_BX + i] = (TP)BnL;
+        uaL[C_BX + t1] = V.Bt1aL;
+        uaL[C_BX + t2] = V.Bt2aL;
+        uaL[C_D] = V.DaL;
+        uaL[C_TAU] = V.TauaL;
+        uaL[C_SX + i] = V.SaL;
+        uaL[C_SX + t1] = V.St1aL;
+        uaL[C_SX + t2] = V.St2aL;
+        uaR[C_BX + i] = (TP)BnR;
+        uaR[C_BX + t1] = V.Bt1aR;
+        uaR[C_BX + t2] = V.Bt2aR;
+        uaR[C_D] = V.DaR;
+        uaR[C_TAU] = V.TauaR;
+        uaR[C_SX + i] = V.SaR;
+        uaR[C_SX + t1] = V.St1aR;
+        uaR[C_SX + t2] = V.St2aR;
+        // region selection at xi = 0 (hlld.py:1447-1480)
+        const TP vi = TP(0);
+        const TP lC = vc;
+        const bool cL_mask = vi <= -pcm;
+        const bool caL_mask = (-pcm < vi) && (vi <= laL);
+        const bool ccL_mask = (laL < vi) && (vi < lC);
+        const bool ccR_mask = (lC <= vi) && (vi < laR);
+        const bool caR_mask = (laR <= vi) && (vi < pcx);
+        const bool cR_mask = vi >= pcx;
+        // the contact states are needed only in the contact regions
+        const bool need_c = ccL_mask || ccR_mask;
+        TP ucD_L = TP(0), ucD_R = TP(0), ucT_L = TP(0), ucT_R = TP(0);
+        TP faTL = TP(0), faTR = TP(0);
+        if (need_c) {
+            faTL = (TP)ph.L.f[C_TAU] + (-pcm) * (uaL[C_TAU] - (TP)ph.L.u[C_TAU]);
+            faTR = (TP)ph.R.f[C_TAU] + (pcx) * (uaR[C_TAU] - (TP)ph.R.u[C_TAU]);
+            ucD_L = uaL[C_D] * sdiv(laL - V.vaL, laL - vc);
+            ucD_R = uaR[C_D] * sdiv(laR - V.vaR, laR - vc);
+            ucT_L = sdiv(laL * uaL[C_TAU] - faTL + p_star * vc - vBc * Bc[i], laL - vc);
+            ucT_R = sdiv(laR * uaR[C_TAU] - faTR + p_star * vc - vBc * Bc[i], laR - vc);
+        }
+#pragma unroll
+        for (int k = 0; k < NCONS; ++k) {
+            const TP fLk = (TP)ph.L.f[k], fRk = (TP)ph.R.f[k];
+            const TP uLk = (TP)ph.L.u[k], uRk = (TP)ph.R.u[k];
+            const TP faLk = fLk + (-pcm) * (uaL[k] - uLk);
+            const TP faRk = fRk + (pcx) * (uaR[k] - uRk);
+            TP ucLk = TP(0), ucRk = TP(0);
+            if (need_c) {
+                if (k == C_D) {
+                    ucLk = ucD_L;
+                    ucRk = ucD_R;
+                } else if (k == C_TAU) {
+                    ucLk = ucT_L;
+                    ucRk = ucT_R;
+                } else if (k >= C_BX) {
+                    ucLk = Bc[k - C_BX];
+                    ucRk = Bc[k - C_BX];
+                } else {
+                    const int cc = k - C_SX;
+                    ucLk = (ucT_L + p_star + ucD_L) * vcomp[cc] - vBc * Bc[cc];
+                    ucRk = (ucT_R + p_star + ucD_R) * vcomp[cc] - vBc * Bc[cc];
+                }
+            }
+            TP f = (TP)fH[k];
+            if (cL_mask) f = fLk;
+            if (caL_mask) f = faLk;
+            if (ccL_mask) f = faLk + laL * (ucLk - uaL[k]);
+            if (ccR_mask) f = faRk + laR * (ucRk - uaR[k]);
+            if (caR_mask) f = faRk;
+            if (cR_mask) f = fRk;
+            o.F[k] = (T)f;
+            if (want_u) {
+                TP u = (TP)uH[k];
+                if (cL_mask) u = uLk;
+                if (caL_mask) u = uaL[k];
+                if (ccL_mask) u = ucLk;
+                if (ccR_mask) u = ucRk;
+                if (caR_mask) u = uaR[k];
+                if (cR_mask) u = uRk;
+                o.U[k] = (T)u;
+            }
+        }
+        o.pstar = (T)p_star;
+    }
+    o.err = err;
+    o.iters = iters_used;
+    o.flags = (uint8_t)((wave_order_bad ? RF_WAVE_ORDER_BAD : 0) | (bn_zero ? RF_BN_ZERO : 0) |
+                        (failed ? RF_FAILED : 0));
+}
+
+}  // namespace hlld

@@ -1,0 +1,4 @@
+// FP64 variant built with -fmad=false: one rounding per operation, in the
+// reference's operation order.
+#define HLLD_NS v_exact
+#include "kernels_impl.cuh"

@@ -1,0 +1,50 @@
+// Launchers exported by each arithmetic variant of kernels_impl.cuh.
+// v_fp64: FP64 with FMA contraction; v_exact: FP64 with one rounding per
+// operation (translation unit built with -fmad=false).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "hlld_b200.h"
+
+namespace hlld {
+
+// Scratch arrays of one 2D step (carved out of the caller's buffer).
+struct Scratch2D {
+    double *Fx[7];  // x-face fluxes: D, Sx, Sy, Sz, tau, Bz, By
+    double *Fy[7];  // y-face fluxes: D, Sx, Sy, Sz, tau, Bz, Bx
+    double *Ez;     // corner EMF
+    double *U0[6];  // RK stage-0 copy of the evolved cell variables
+    double *Bx0, *By0;
+    hlld_step_diag_t *diag;  // used when the caller passes none
+};
+
+#define HLLD_DECLARE_VARIANT(NS)                                                                  \
+    namespace NS {                                                                                \
+    void launch_riemann_faces(int64_t n, const void *const *sL, const void *const *sR, int idir,  \
+                              int solver, double gamma, void *const *F, void *const *U,           \
+                              void *pstar, int32_t *err, int32_t *iters, uint8_t *flags,          \
+                              hlld_flux_diag_t *diag, cudaStream_t st);                           \
+    void launch_cons_to_prim(int64_t n, const void *const *cons, double gamma, double atmo_rho,   \
+                             double atmo_eps, void *const *prim, uint8_t *status,                 \
+                             cudaStream_t st);                                                    \
+    void launch_prim_to_cons(int64_t n, const void *const *prim, void *const *cons,               \
+                             cudaStream_t st);                                                    \
+    void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,      \
+                           hlld_step_diag_t *diag, cudaStream_t st);                              \
+    void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,  \
+                           double dt_host, const double *dt_dev, int scheme,                      \
+                           hlld_step_diag_t *diag, cudaStream_t st);                              \
+    void launch_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,        \
+                              double *dt_dev, unsigned long long *work, cudaStream_t st);         \
+    void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis,                \
+                        double *const *F, hlld_flux_diag_t *fdiag, cudaStream_t st);              \
+    void launch_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,  \
+                            const hlld_step_diag_t *diag, int stage, int scheme, double dt_host,  \
+                            const double *dt_dev, cudaStream_t st);                               \
+    }
+
+HLLD_DECLARE_VARIANT(v_fp64)
+HLLD_DECLARE_VARIANT(v_exact)
+
+}  // namespace hlld

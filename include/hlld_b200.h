@@ -1,0 +1,190 @@
+/*
+ * hlld_b200 C ABI: B200 (sm_100a) kernels for the special-relativistic MHD
+ * finite-volume step of kemi2805/HLLD-AI (HLLE/HLLD fluxes, Kastaun C2P,
+ * PLM/WENO5-Z/MP5 reconstruction, constrained transport, SSP-RK2/3).
+ *
+ * Conventions
+ *   - All array arguments are DEVICE pointers to contiguous row-major
+ *     arrays; no entry point allocates device memory except where stated.
+ *   - Real arrays are double for HLLD_FP64 / HLLD_FP64_EXACT; for
+ *     HLLD_MIXED the primitive arrays are float and everything else double
+ *     (see each entry point).
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Every
+ *     entry point only enqueues work; nothing synchronises the host.
+ *   - Return value: HLLD_OK or a negative HLLD_ERR_* code;
+ *     hlld_error_string() names it and hlld_last_error_detail() gives the
+ *     last failure's message.  Numeric failures (non-converged roots,
+ *     fallbacks) are never errors: they are reported in status/flag arrays
+ *     and device counters, as the reference reports them in masks.
+ *
+ * 2D layout (src/physics/grid.py:146-207): cells (nxt, nyt) with
+ * nxt = nx + 2 ng, x-major (y contiguous); Bxf (nxt+1, nyt) lower-x faces;
+ * Byf (nxt, nyt+1) lower-y faces; corner EMF (nxt+1, nyt+1).
+ */
+#ifndef HLLD_B200_H
+#define HLLD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HLLD_OK 0
+#define HLLD_ERR_INVALID (-1)     /* bad argument: shape, enum, null pointer */
+#define HLLD_ERR_CUDA (-2)        /* a CUDA launch or runtime call failed */
+#define HLLD_ERR_UNSUPPORTED (-3) /* valid but not implemented here */
+#define HLLD_ERR_SCRATCH (-4)     /* scratch buffer too small */
+
+enum hlld_precision {
+    HLLD_FP64 = 0,       /* FP64 throughout, FMA contraction on */
+    HLLD_FP64_EXACT = 1, /* FP64, one rounding per operation (reference order) */
+    HLLD_MIXED = 2       /* FP32 reconstruction/fluxes/update, FP64 C2P, p*, RK state */
+};
+enum hlld_solver { HLLD_SOLVER_HLLE = 0, HLLD_SOLVER_HLLD = 1 };
+enum hlld_limiter {
+    HLLD_LIM_PCM = 0, HLLD_LIM_MC = 1, HLLD_LIM_MINMOD = 2,
+    HLLD_LIM_WENO5Z = 3, HLLD_LIM_MP5 = 4, HLLD_LIM_MP7 = 5
+};
+enum hlld_bc { HLLD_BC_OUTFLOW = 0, HLLD_BC_PERIODIC = 1 };
+
+/* C2P status bits (src/physics/c2p.py:290-294, :360-362) */
+#define HLLD_ST_BRACKET_OK 1u
+#define HLLD_ST_CONVERGED 2u
+#define HLLD_ST_V_CLAMPED 4u
+#define HLLD_ST_ATMO 8u
+#define HLLD_ST_BISECTED 16u
+/* Riemann-solver flags (src/physics/hlld.py:1487-1513) */
+#define HLLD_RF_WAVE_ORDER_BAD 1u
+#define HLLD_RF_BN_ZERO 2u
+#define HLLD_RF_FAILED 4u
+
+/* Device-resident counters of one flux sweep: the numbers the reference
+ * keeps in hlld.LAST_DIAG (src/physics/hlld.py:1516-1529). */
+typedef struct {
+    unsigned long long n_faces;
+    unsigned long long n_not_converged;
+    unsigned long long n_wave_order_bad;
+    unsigned long long n_bn_zero;
+    unsigned long long n_failed;
+    unsigned long long iters_sum_conv; /* sum of p* iterations over converged faces */
+    unsigned long long n_conv;
+    unsigned long long max_iters;
+    unsigned long long fd_max_bits; /* bits of max |F_D| (non-negative double) */
+} hlld_flux_diag_t;
+
+/* Device-resident counters of one RK step (last stage's sweeps, as the
+ * reference's rk_step_ct returns, src/physics/driver2d.py:441-448). */
+typedef struct {
+    hlld_flux_diag_t sweep[2];
+    unsigned long long c2p_not_converged;
+    unsigned long long c2p_bisected;
+    unsigned long long c2p_atmo;
+    unsigned long long c2p_bad_bracket;
+    unsigned long long speed_max_bits[2]; /* bits of max(|v_d| + c_f), physical cells */
+} hlld_step_diag_t;
+
+typedef struct {
+    int32_t nx, ny, ng;
+    double dx, dy;
+    int32_t bc_x, bc_y;   /* enum hlld_bc */
+    int32_t limiter;      /* enum hlld_limiter */
+    int32_t solver;       /* enum hlld_solver */
+    double gamma;         /* ideal gas: hybrid_eos(K=0, gamma, gamma_th=gamma) */
+    double atmo_rho;
+    int32_t upwind;       /* Gardiner-Stone upwinded corner EMF (1) or flux-CT (0) */
+    int32_t precision;    /* enum hlld_precision */
+} hlld_grid2d_t;
+
+/* State2D (src/physics/state.py:54-74) as device pointers.
+ * cons: D, Sx, Sy, Sz, tau, Bz (state.py:41 EVOLVED_KEYS), double.
+ * prims: rho, vx, vy, vz, p, eps, Bx, By, Bz (double, float for HLLD_MIXED). */
+typedef struct {
+    void *cons[6];
+    void *Bxf;
+    void *Byf;
+    void *prims[9];
+} hlld_state2d_t;
+
+int hlld_version(void);
+const char *hlld_error_string(int code);
+const char *hlld_last_error_detail(void);
+
+/* Replaces src/physics/hlld.py:185-217 primitive_to_conserved.
+ * prim: 9 arrays (rho, vx, vy, vz, p, eps, Bx, By, Bz); cons: 8 arrays
+ * (D, Sx, Sy, Sz, tau, Bx, By, Bz); double (precision FP64 / FP64_EXACT). */
+int hlld_prim_to_cons(int64_t n, const void *const *prim, int precision, void *const *cons,
+                      void *stream);
+
+/* Replaces src/physics/c2p.py:313-363 conservative_to_primitive (Kastaun
+ * master function, mu_+ bisection, bracketed secant, bisection continuation,
+ * atmosphere floor).  status (may be NULL): HLLD_ST_* bits per element. */
+int hlld_cons_to_prim(int64_t n, const void *const *cons, double gamma, double atmo_rho,
+                      double atmo_eps, int precision, void *const *prim, uint8_t *status,
+                      void *stream);
+
+/* Replaces the flux_fn plugin contract flux_fn(sL, sR, eos, idir) ->
+ * (F, U, p_star): src/physics/hlld.py:1005-1044 hlle_flux and
+ * src/physics/hlld.py:1202-1543 hlld_flux, on n flattened faces.
+ * sL, sR: 9 primitive arrays each; F, U: 8 conserved arrays each (U may be
+ * NULL); pstar (p* < 0 marks an HLLE fallback face, hlld.py:1531);
+ * err / iters / flags may be NULL; diag (may be NULL) is zeroed and filled
+ * with the LAST_DIAG counters. */
+int hlld_riemann_faces(int64_t n, const void *const *sL, const void *const *sR, int idir,
+                       int solver, double gamma, int precision, void *const *F, void *const *U,
+                       void *pstar, int32_t *err, int32_t *iters, uint8_t *flags,
+                       hlld_flux_diag_t *diag, void *stream);
+
+/* Bytes of scratch hlld_rk_step_ct needs for grid g (face fluxes, corner
+ * EMF, the RK stage-0 copy). */
+int hlld_step2d_scratch_bytes(const hlld_grid2d_t *g, size_t *bytes);
+
+/* Replaces src/physics/driver2d.py:420-448 rk_step_ct (with ct_stage
+ * :361-392, sweep.py:30-135, ct.py:44-199, state.py:77-103 combine and
+ * sync_state :395-417): one SSP-RK2 (scheme 2) or RK3 (scheme 3) step with
+ * constrained transport, in place on s.  dt is read from dt_dev when it is
+ * not NULL (device scalar, lets the step be graph-captured), else dt_host.
+ * diag (device, may be NULL) is zeroed and filled. */
+int hlld_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scratch,
+                    size_t scratch_bytes, double dt_host, const double *dt_dev, int scheme,
+                    hlld_step_diag_t *diag, void *stream);
+
+/* Replaces src/physics/driver2d.py:395-417 sync_state: face BCs, cell BCs,
+ * cell-centred B, C2P of the physical cells, primitive BCs, in place.
+ * status (nxt*nyt, may be NULL) gets HLLD_ST_* bits of the physical cells. */
+int hlld_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
+                    hlld_step_diag_t *diag, void *stream);
+
+/* Replaces src/physics/sweep.py:30-119 sweep() in the form the 2D step uses
+ * it (reconstruct_prims, normal B taken from the staggered faces
+ * sweep.py:82-89, flux_fn on every face, F[B_n] = 0 sweep.py:99-100), fused
+ * into one launch.  F: 7 face arrays D, Sx, Sy, Sz, tau, Bz, B_t with B_t =
+ * By for axis 0 and Bx for axis 1 ((nxt+1, nyt) or (nxt, nyt+1)); the zero
+ * normal-B flux is not stored.  diag (device, required) is zeroed, then
+ * receives the LAST_DIAG counters and max |F_D|. */
+int hlld_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
+                 hlld_flux_diag_t *diag, void *stream);
+
+/* Replaces the rest of ct_stage + combine for RK stage `stage` (0-based) of
+ * `scheme` (src/physics/driver2d.py:382-391, :440-445; ct.py:57-185;
+ * sweep.py:122-135; state.py:77-103): corner EMF, flux divergence, CT face
+ * update and the SSP-RK combine, in place on s.  Fx, Fy: the two sweeps'
+ * outputs; Ez: (nxt+1)(nyt+1) work array; U0 (6 cell arrays), Bx0, By0: the
+ * RK stage-0 copy, written at stage 0 and read afterwards; diag: the step
+ * counters whose sweep[0/1].fd_max_bits set the upwind deadband (ct.py:114). */
+int hlld_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *const *Fx,
+                     void *const *Fy, void *Ez, void *const *U0, void *Bx0, void *By0,
+                     const hlld_step_diag_t *diag, int stage, int scheme, double dt_host,
+                     const double *dt_dev, void *stream);
+
+/* Replaces src/physics/driver2d.py:251-281 compute_dt_2d: writes
+ * dt = cfl / (max(|vx|+cf)/dx + max(|vy|+cf)/dy) to dt_dev (device double);
+ * work (device, >= 2 unsigned long long) holds the running maxima. */
+int hlld_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,
+                       double *dt_dev, unsigned long long *work, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

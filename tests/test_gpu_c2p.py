@@ -1,0 +1,84 @@
+"""Kastaun C2P kernel against the oracle and as a P2C -> C2P round trip
+(reference tests/test_c2p.py:109-244, with the hot path's ideal-gas EOS)."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import bitwise_equal, max_rel, random_prims, to_dev, to_np
+from oracle import oracle
+
+import hlld_ai_b200 as H
+
+GAMMA = 5.0 / 3.0
+EOS = H.hybrid_eos(K=0.0, gamma=GAMMA, gamma_th=GAMMA)
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "hydro": dict(zero_B=True, seed=1),
+    "mhd": dict(B_mag=5.0, seed=3),
+    "W12": dict(W_range=(1.0, 2.0), B_mag=3.0, seed=5),
+    "W2_10": dict(W_range=(2.0, 10.0), B_mag=3.0, seed=6),
+    "low_rho": dict(rho_range=(1e-8, 1e-4), B_mag=0.1, seed=7),
+    "B_dominated": dict(rho_range=(1e-3, 1e-1), B_mag=20.0, seed=8),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_c2p_exact_bitwise_and_roundtrip(case):
+    prims = random_prims(2000, GAMMA, **CASES[case])
+    cons_np = oracle.prim_to_cons(to_np(prims))
+    cons = H.primitive_to_conserved(to_dev(to_np(prims)), precision="fp64_exact")
+    for k in cons_np:
+        assert bitwise_equal(cons[k].cpu().numpy(), cons_np[k]), ("p2c", k)
+    out, st = H.conservative_to_primitive(to_dev(cons_np), EOS, atmo_rho=1e-12,
+                                          return_status=True, precision="fp64_exact")
+    o, ost = oracle.cons_to_prim(cons_np, GAMMA, atmo_rho=1e-12)
+    for k in o:
+        assert bitwise_equal(out[k].cpu().numpy(), o[k]), ("c2p", k)
+    assert np.array_equal(st["converged"].cpu().numpy(), (ost & oracle.ST_CONVERGED) != 0)
+    # round trip at the reference's tolerances (test_c2p.py:130-170)
+    tol = 1e-5 if case in ("W2_10", "low_rho", "B_dominated") else 1e-6
+    rho_in = prims["rho"].numpy()
+    assert np.max(np.abs(o["rho"] - rho_in) / rho_in) < tol
+    for k in ("vx", "vy", "vz"):
+        assert np.max(np.abs(o[k] - prims[k].numpy())) < tol
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_c2p_fma_build_close_to_oracle(case):
+    prims = random_prims(2000, GAMMA, **CASES[case])
+    cons_np = oracle.prim_to_cons(to_np(prims))
+    out = H.conservative_to_primitive(to_dev(cons_np), EOS, atmo_rho=1e-12)
+    o, _ = oracle.cons_to_prim(cons_np, GAMMA, atmo_rho=1e-12)
+    for k in ("rho", "p", "eps"):
+        rel = np.abs(out[k].cpu().numpy() - o[k]) / np.maximum(np.abs(o[k]), 1e-300)
+        assert rel.max() < 1e-9, (case, k, rel.max())
+
+
+def test_hot_fast_gas_uses_the_continuation():
+    """reference tests/test_c2p.py:303-333: hot fast gas converges only
+    through the bisection continuation."""
+    import math
+    b = 0.5 * math.cos(math.radians(45))
+    t = lambda *v: np.array(v, dtype=np.float64)
+    prims = {"rho": t(0.1, 0.1, 0.5, 0.1, 0.1, 1.0, 10.0, 0.22),
+             "p": t(1.0, 0.01, 1.0, 1.0, 1.0, 1.0, 1.0, 0.13),
+             "vx": t(0.99, 0.0, 0.0, 0.0, 0.99, 0.3, 0.995, 0.7),
+             "vy": t(0.0, 0.0, 0.0, 0.99, 0.0, 0.1, 0.0, 0.7),
+             "vz": t(0, 0, 0, 0, 0, 0, 0, 0),
+             "Bx": t(b, b, b, b, 0.0, 0.5, 1.0, 0.28), "By": t(b, b, b, b, 0.0, 0.0, 0.0, 0.28),
+             "Bz": t(0, 0, 0, 0, 0, 0, 0, 0)}
+    prims["eps"] = 0.0 + (prims["p"] - 0.0) / (prims["rho"] * (GAMMA - 1.0))
+    cons = oracle.prim_to_cons(prims)
+    out, st = H.conservative_to_primitive(to_dev(cons), EOS, return_status=True)
+    raw = H.conservative_to_primitive(to_dev(cons), EOS, return_status=False)
+    assert bool(st["converged"].all())
+    for k in ("rho", "p"):
+        rel = np.abs(out[k].cpu().numpy() - prims[k]) / np.abs(prims[k])
+        assert rel.max() < 1e-9, (k, rel)
+    for k in ("vx", "vy"):
+        assert np.abs(out[k].cpu().numpy() - prims[k]).max() < 1e-10
+    o, ost = oracle.cons_to_prim(cons, GAMMA)
+    assert ost[0] & oracle.ST_BISECTED
+    for k in o:
+        assert bitwise_equal(raw[k].cpu().numpy(), o[k]) or max_rel(o[k], raw[k].cpu().numpy()) < 1e-12
