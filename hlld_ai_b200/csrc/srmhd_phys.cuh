@@ -196,7 +196,7 @@ template <typename T> struct Kastaun {
     // exactly 2^-k after k halvings, so the batch early stop never fires
     // early).  f_a(mu_lo) is a deterministic function of mu_lo, so the value
     // from the previous iteration is reused instead of re-evaluated.
-    __device__ __forceinline__ T mu_plus() const {
+    __device__ __forceinline__ T mu_plus_bisect() const {
         T lo = T(0), hi = T(1) / (T(1) + K<T>::tiny);
         T f_lo = fa(lo);
 #pragma unroll 1
@@ -212,6 +212,78 @@ template <typename T> struct Kastaun {
             }
         }
         return hi;
+    }
+
+    // The same 50 halvings, evaluating f_a only where its sign is in doubt.
+    //
+    // f_a(mu) = mu sqrt(1 + rbar2(mu)) - 1 is strictly increasing: with
+    // chi = 1/(1 + mu b), rbar2 = c/b + (r^2 - c/b) chi^2 (b = |B~|^2,
+    // c = (B~.r)^2), so mu^2 (1 + rbar2) = mu^2 (1 + c/b) + (r^2 - c/b) (mu chi)^2
+    // has derivative 2 mu [(1 + c/b) + (r^2 - c/b) chi^3] > 0 whenever the
+    // rounding-level violation of r^2 >= c/b is below 1 + c/b (|r|^2 < 1e12
+    // here).  Its evaluation is accurate to ~1e-15 absolute near the root
+    // (all terms positive, the final x - 1 exact).  So once a root estimate r
+    // is confirmed by f_a(r - d) < -8e-15 and f_a(r + d) > 8e-15, every
+    // midpoint below r - d evaluates negative and every midpoint above
+    // r + d non-negative, and the bisection's decision there is known
+    // without evaluating.  With f_a(0) = -1 < 0 the reference's test
+    // f_lo * f_mid <= 0 is f_mid >= 0 (|f_a| >= 2^-53 or 0 near the root, so
+    // the product cannot underflow); a NaN f_mid freezes hi for good, as
+    // in the reference.  Anything outside these conditions runs the plain
+    // loop.  The result is the plain loop's bit for bit.
+    __device__ __forceinline__ T mu_plus() const {
+        if constexpr (sizeof(T) == 8) {
+            if (!(rNorm2 < T(1e12)) || !(BtNorm2 < T(1e300)) || !(fa(T(0)) < T(0)))
+                return mu_plus_bisect();
+            // root of g(mu) = mu^2 (1 + rbar2(mu)) - 1 by safeguarded Newton
+            const T b = BtNorm2, c = B_dot_r * B_dot_r, rN = rNorm2;
+            T m0 = T(0), m1 = T(1);
+            T mu = T(1) / sqrt(T(1) + rN);
+#pragma unroll 1
+            for (int it = 0; it < 60; ++it) {
+                T ch = T(1) / (T(1) + mu * b);
+                T dch = -b * ch * ch;
+                T rb = rN * ch * ch + mu * ch * (T(1) + ch) * c;
+                T drb = rN * T(2) * ch * dch + c * ((ch + mu * dch) * (T(1) + ch) + mu * ch * dch);
+                T g = mu * mu * (T(1) + rb) - T(1);
+                T dg = T(2) * mu * (T(1) + rb) + mu * mu * drb;
+                if (g < T(0)) m0 = mu;
+                else m1 = mu;
+                if (g == T(0)) break;
+                T nm = mu - g / dg;
+                if (!(nm > m0 && nm < m1)) nm = T(0.5) * (m0 + m1);
+                T stp = fabs(nm - mu);
+                mu = nm;
+                if (stp <= T(2e-16) * mu) break;
+            }
+            const T r = mu;
+            T d = T(1e-13) * r;
+            bool ok = false;
+#pragma unroll 1
+            for (int t = 0; t < 4 && !ok; ++t) {
+                ok = (fa(r - d) < T(-8e-15)) && (fa(r + d) > T(8e-15));
+                if (!ok) d *= T(32);
+            }
+            if (!ok) return mu_plus_bisect();
+            T lo = T(0), hi = T(1) / (T(1) + K<T>::tiny);
+#pragma unroll 1
+            for (int it = 0; it < K<T>::mu_plus_iters; ++it) {
+                T mid = T(0.5) * (lo + hi);
+                if (mid < r - d) {
+                    lo = mid;
+                } else if (mid > r + d) {
+                    hi = mid;
+                } else {
+                    T f_mid = fa(mid);
+                    if (isnan(f_mid)) break;
+                    if (f_mid >= T(0)) hi = mid;
+                    else lo = mid;
+                }
+            }
+            return hi;
+        } else {
+            return mu_plus_bisect();
+        }
     }
 };
 
