@@ -10,7 +10,8 @@ import os
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libhlld_b200.so")
+# HLLD_B200_LIB overrides the library path (e.g. an alternative build)
+LIB_PATH = os.environ.get("HLLD_B200_LIB") or os.path.join(HERE, "libhlld_b200.so")
 
 HLLD_OK = 0
 FP64, FP64_EXACT, MIXED = 0, 1, 2

