@@ -27,6 +27,7 @@ UNITS = [
     ("capi.cu", []),
     ("variant_fp64.cu", []),
     ("variant_exact.cu", ["-fmad=false"]),
+    ("noalloc.cu", []),
 ]
 
 

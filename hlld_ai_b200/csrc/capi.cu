@@ -92,6 +92,14 @@ size_t layout_scratch(const hlld_grid2d_t *g, char *base, hlld::Scratch2D *sc) {
 
 }  // namespace
 
+int hlld::report_error(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_detail, sizeof g_detail, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
 extern "C" {
 
 int hlld_version(void) { return 1; }

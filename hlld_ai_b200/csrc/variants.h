@@ -44,6 +44,9 @@ struct Scratch2D {
                             const double *dt_dev, cudaStream_t st);                               \
     }
 
+// Records the detail string hlld_last_error_detail() returns; returns code.
+int report_error(int code, const char *fmt, ...);
+
 HLLD_DECLARE_VARIANT(v_fp64)
 HLLD_DECLARE_VARIANT(v_exact)
 

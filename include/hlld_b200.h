@@ -150,6 +150,19 @@ int hlld_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scrat
                     size_t scratch_bytes, double dt_host, const double *dt_dev, int scheme,
                     hlld_step_diag_t *diag, void *stream);
 
+/* No counterpart in the reference.  hlld_rk_step_ct for callers that cannot
+ * allocate device memory: code running inside CUDA stream capture (cudaMalloc
+ * is not allowed there), and hosts whose device memory belongs to a pool or
+ * allocator they do not control.  The scratch is a 64 MiB static device
+ * array inside the library (held on every GPU that loads it until exit), so
+ * grids whose hlld_step2d_scratch_bytes exceeds 64 MiB (square grids above 599^2 cells
+ * with ng = 2) get HLLD_ERR_SCRATCH.  Calls that overlap on the GPU share the
+ * array and race; the first call on a device looks the array up (make it
+ * before any stream capture).  Allocates nothing. */
+int hlld_rk_step_ct_static(const hlld_grid2d_t *g, const hlld_state2d_t *s, double dt_host,
+                           const double *dt_dev, int scheme, hlld_step_diag_t *diag,
+                           void *stream);
+
 /* Replaces src/physics/driver2d.py:395-417 sync_state: face BCs, cell BCs,
  * cell-centred B, C2P of the physical cells, primitive BCs, in place.
  * status (nxt*nyt, may be NULL) gets HLLD_ST_* bits of the physical cells. */
