@@ -1,16 +1,19 @@
 """Benchmark: 2D magnetic rotor, HLLD + PLM(MC) + SSP-RK3 + CT, zone-updates/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--n 2048] [--precision fp64|fp64_exact]
+                    [--n 2048] [--precision mixed|fp64|fp64_exact]
 
 One step is one full SSP-RK3 step (three stages, each: x and y sweeps, corner
 EMF + update, sync) of the periodic tapered rotor on [0,1]^2 at n^2 cells,
 preceded by the on-device CFL time step, with the state resident in HBM
-(1.5 GB at 2048^2, far above the 126 MB L2, so no flush is needed).  The
-line printed by rank 0 also carries the end-to-end rate through the public
-API with the state copied host -> device and back every step, the roofline
-of the dominant kernel (the fused sweep), the CPU baseline (the C oracle on
-the host cores) and the SM clocks sampled during the timed region.
+(over 1 GB at 2048^2, far above the 126 MB L2, so no flush is needed).
+`value` is the mixed-precision step (FP32 reconstruction/fluxes/update, FP64
+C2P, p* iteration and RK state); the line also carries the FP64 step's rate
+and the mixed-vs-FP64 density L1/Linf after the timed number of steps (same
+dt sequence), the end-to-end rate through the public API with the state
+copied host -> device and back every step, the roofline of the dominant
+kernel (the fused sweep), the CPU baseline (the C oracle on the host cores)
+and the SM clocks sampled during the timed region.
 
 N > 1 (torchrun): every rank advances its own rotor replica (the reference
 path has no domain decomposition; replicas only) and the rate is the sum
@@ -46,7 +49,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=2048)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_exact"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "fp64_exact"])
+    ap.add_argument("--no-fp64-arm", action="store_true",
+                    help="skip timing the FP64 step and the mixed-vs-FP64 L1 check")
     ap.add_argument("--cfl", type=float, default=0.4)
     ap.add_argument("--cpu-n", type=int, default=512, help="grid of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -172,12 +177,128 @@ def run_reference(a):
 
 # ── our arm ──────────────────────────────────────────────────────────────────
 
-def run_ours(a):
+def _timed_rotor(a, precision, dev, world, record=True):
+    """Set up the rotor at a.n^2 in `precision`, run a.warmup steps, then time
+    a.steps steps between CUDA events; returns a dict of results."""
     import torch
     import torch.distributed as dist
 
     import hlld_ai_b200 as H
     from hlld_ai_b200 import _lib
+
+    g, eos, st, spec = H.setup_problem(PROBLEM, a.n, limiter="mc", device=dev,
+                                       precision=precision)
+    stepper = H.Stepper2D(g, eos, bc_x=spec["bc"][0], bc_y=spec["bc"][1], flux_fn="hlld",
+                          limiter="mc", precision=precision)
+    s = stepper._struct(st)
+    gc = stepper.gc
+    L = _lib.lib()
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    # component buffers of the instrumented step (same kernels as hlld_rk_step_ct)
+    nfx, nfy = (g.nxt + 1) * g.nyt, g.nxt * (g.nyt + 1)
+    rdt = torch.float32 if precision == "mixed" else torch.float64
+    f64 = dict(dtype=torch.float64, device=dev)
+    Fx = [torch.empty(nfx, dtype=rdt, device=dev) for _ in range(7)]
+    Fy = [torch.empty(nfy, dtype=rdt, device=dev) for _ in range(7)]
+    Ez = torch.empty((g.nxt + 1) * (g.nyt + 1), dtype=rdt, device=dev)
+    U0 = [torch.empty(g.nxt * g.nyt, **f64) for _ in range(6)]
+    Bx0, By0 = torch.empty(nfx, **f64), torch.empty(nfy, **f64)
+    diag = torch.zeros(ctypes.sizeof(_lib.StepDiag), dtype=torch.uint8, device=dev)
+    fd_off = ctypes.sizeof(_lib.FluxDiag)
+    pFx, pFy, pU0 = _lib.ptr_array(Fx), _lib.ptr_array(Fy), _lib.ptr_array(U0)
+    dt = stepper.dt_buf
+    sweep_events = []
+
+    def step(rec=False):
+        stepper.compute_dt(st, a.cfl, out=dt)
+        for stage in range(3):
+            for axis, pF in ((0, pFx), (1, pFy)):
+                if rec:
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                _lib.check(L.hlld_sweep2d(ctypes.byref(gc), ctypes.byref(s), axis, pF,
+                                          diag.data_ptr() + axis * fd_off, sh), "sweep2d")
+                if rec:
+                    e1.record(stream)
+                    sweep_events.append((e0, e1))
+            _lib.check(L.hlld_ct_update2d(ctypes.byref(gc), ctypes.byref(s), pFx, pFy,
+                                          Ez.data_ptr(), pU0, Bx0.data_ptr(), By0.data_ptr(),
+                                          diag.data_ptr(), stage, 3, 0.0, dt.data_ptr(), sh),
+                       "ct_update2d")
+            _lib.check(L.hlld_sync_state(ctypes.byref(gc), ctypes.byref(s), None, None, sh),
+                       "sync_state")
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(dev.index or 0) if record else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(a.steps):
+        step(rec=True)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        m = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        ms = float(m.item())
+    sweep_ms = [e0.elapsed_time(e1) for e0, e1 in sweep_events]
+    return dict(g=g, eos=eos, st=st, spec=spec, stepper=stepper, ms=ms, sweep_ms=sweep_ms,
+                clocks=clk, faces=(nfx + nfy) / 2.0,
+                value=world * g.nx * g.ny * a.steps / (ms * 1e-3))
+
+
+def _l1_mixed_vs_fp64(a, dev, steps):
+    """Density L1 (mean |rho_mixed - rho_fp64| over physical cells) after
+    `steps` RK3 steps from the same initial state with the FP64 run's dt."""
+    import torch
+
+    import hlld_ai_b200 as H
+
+    res = {}
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        g, eos, st, spec = H.setup_problem(PROBLEM, a.n, limiter="mc", device=dev, precision=prec)
+        runs[prec] = (g, st, H.Stepper2D(g, eos, bc_x=spec["bc"][0], bc_y=spec["bc"][1],
+                                         flux_fn="hlld", limiter="mc", precision=prec))
+    g = runs["fp64"][0]
+    for _ in range(steps):
+        dt = float(runs["fp64"][2].compute_dt(runs["fp64"][1], a.cfl).item())
+        for prec in ("fp64", "mixed"):
+            runs[prec][2].step(runs[prec][1], dt, "rk3")
+    ph = g.phys
+    r64 = runs["fp64"][1].prims["rho"][ph]
+    rmx = runs["mixed"][1].prims["rho"][ph].double()
+    d = (rmx - r64).abs()
+    res["l1_rho"] = float(d.mean())
+    res["linf_rho"] = float(d.max())
+    res["l1_rho_rel"] = float(d.mean() / r64.abs().mean())
+    res["steps"] = steps
+    del runs
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    import hlld_ai_b200 as H
     from hlld_ai_b200.physics.state import EVOLVED_KEYS, PRIM_KEYS
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -189,90 +310,39 @@ def run_ours(a):
         dist.init_process_group("nccl", device_id=dev,
                                 timeout=__import__("datetime").timedelta(seconds=300))
 
-    g, eos, st, spec = H.setup_problem(PROBLEM, a.n, limiter="mc", device=dev,
-                                       precision=a.precision)
-    stepper = H.Stepper2D(g, eos, bc_x=spec["bc"][0], bc_y=spec["bc"][1], flux_fn="hlld",
-                          limiter="mc", precision=a.precision)
-    s = stepper._struct(st)
-    gc = stepper.gc
-    L = _lib.lib()
-    stream = torch.cuda.current_stream(dev)
-    sh = stream.cuda_stream
-
-    # component buffers of the instrumented step (same kernels as hlld_rk_step_ct)
-    nfx, nfy = (g.nxt + 1) * g.nyt, g.nxt * (g.nyt + 1)
-    f64 = dict(dtype=torch.float64, device=dev)
-    Fx = [torch.empty(nfx, **f64) for _ in range(7)]
-    Fy = [torch.empty(nfy, **f64) for _ in range(7)]
-    Ez = torch.empty((g.nxt + 1) * (g.nyt + 1), **f64)
-    U0 = [torch.empty(g.nxt * g.nyt, **f64) for _ in range(6)]
-    Bx0, By0 = torch.empty(nfx, **f64), torch.empty(nfy, **f64)
-    diag = torch.zeros(ctypes.sizeof(_lib.StepDiag), dtype=torch.uint8, device=dev)
-    fd_off = ctypes.sizeof(_lib.FluxDiag)
-    pFx, pFy, pU0 = _lib.ptr_array(Fx), _lib.ptr_array(Fy), _lib.ptr_array(U0)
-    dt = stepper.dt_buf
-    sweep_events = []
-
-    def step(record=False):
-        stepper.compute_dt(st, a.cfl, out=dt)
-        for stage in range(3):
-            for axis, pF in ((0, pFx), (1, pFy)):
-                if record:
-                    e0 = torch.cuda.Event(enable_timing=True)
-                    e1 = torch.cuda.Event(enable_timing=True)
-                    e0.record(stream)
-                _lib.check(L.hlld_sweep2d(ctypes.byref(gc), ctypes.byref(s), axis, pF,
-                                          diag.data_ptr() + axis * fd_off, sh), "sweep2d")
-                if record:
-                    e1.record(stream)
-                    sweep_events.append((e0, e1))
-            _lib.check(L.hlld_ct_update2d(ctypes.byref(gc), ctypes.byref(s), pFx, pFy,
-                                          Ez.data_ptr(), pU0, Bx0.data_ptr(), By0.data_ptr(),
-                                          diag.data_ptr(), stage, 3, 0.0, dt.data_ptr(), sh),
-                       "ct_update2d")
-            _lib.check(L.hlld_sync_state(ctypes.byref(gc), ctypes.byref(s), None,
-                                         None, sh), "sync_state")
-
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    for _ in range(a.steps):
-        step(record=True)
-    t1.record(stream)
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        m = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        ms = float(m.item())
-    zones = g.nx * g.ny
-    value = world * zones * a.steps / (ms * 1e-3)
+    main = _timed_rotor(a, a.precision, dev, world, record=True)
+    g, st, stepper = main["g"], main["st"], main["stepper"]
+    ms, zones = main["ms"], g.nx * g.ny
+    value = main["value"]
+    clk = main["clocks"]
     launches_per_step = 2 + 3 * 9  # speed + dt; per stage 2 sweeps, emf, update, 2 face ghosts, cons ghosts, c2p, prim ghosts
 
     # roofline of the dominant kernel (fused sweep), timed inside the region
-    sweep_ms = [e0.elapsed_time(e1) for e0, e1 in sweep_events]
+    sweep_ms = main["sweep_ms"]
     sweep_avg_s = 1e-3 * sum(sweep_ms) / len(sweep_ms)
-    faces = (nfx + nfy) / 2.0
-    # algorithmic bytes per face: 6 primitives + 2 face-B words read per cell,
-    # 7 flux words written per face (FP64)
-    bytes_per_face = (8 + 7) * 8
-    achieved = bytes_per_face * faces / sweep_avg_s / 1e9
+    rb = 4 if a.precision == "mixed" else 8
+    # algorithmic bytes per face: 6 primitives (R) + 2 face-B words (FP64)
+    # read per cell, 7 flux words (R) written per face
+    bytes_per_face = 6 * rb + 2 * 8 + 7 * rb
+    achieved = bytes_per_face * main["faces"] / sweep_avg_s / 1e9
     peak, peak_kind = peaks()
     sweep_share = sum(sweep_ms) / ms
+
+    fp64_arm = None
+    if a.precision == "mixed" and not a.no_fp64_arm:
+        del main
+        torch.cuda.empty_cache()
+        r64 = _timed_rotor(a, "fp64", dev, world, record=False)
+        fp64_arm = {"value": r64["value"], "ms_per_step": r64["ms"] / a.steps,
+                    "mixed_speedup": value / r64["value"]}
+        del r64
+        torch.cuda.empty_cache()
+        fp64_arm.update(_l1_mixed_vs_fp64(a, dev, a.steps))
+        g, eos, st, spec = H.setup_problem(PROBLEM, a.n, limiter="mc", device=dev,
+                                           precision=a.precision)
+        stepper = H.Stepper2D(g, eos, bc_x=spec["bc"][0], bc_y=spec["bc"][1], flux_fn="hlld",
+                              limiter="mc", precision=a.precision)
+    stream = torch.cuda.current_stream(dev)
 
     # end to end through the public API with host buffers
     e2e = None
@@ -319,17 +389,19 @@ def run_ours(a):
         times = cpu_sample(a.cpu_n, 3, threads)
         cpu = {"value": a.cpu_n ** 2 * len(times) / sum(times), "unit": "zone-updates/s",
                "cores": threads, "kind": "port",
-               "sample": f"3 RK3 steps of the same rotor at {a.cpu_n}^2 (C oracle, {threads} threads)"}
+               "sample": f"3 RK3 steps of the same rotor at {a.cpu_n}^2 (C oracle, FP64, {threads} threads)"}
 
     if rank == 0:
         line = {
             "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
+            "data": "synthetic",
             "config": {"workload": WORKLOAD, "n": a.n, "precision": a.precision,
                        "parallelism": f"replicas x{world}", "cfl": a.cfl,
-                       "l2": "inputs exceed L2 (state 1.5 GB at 2048^2), no flush"},
+                       "l2": "inputs exceed L2 (state >1 GB at 2048^2), no flush"},
+            "fp64": fp64_arm,
             "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps,
             "roofline": {"bound": "hbm", "kernel": "sweep_kernel (x and y)",

@@ -51,6 +51,17 @@ class State2DC(ctypes.Structure):
                 ("prims", ctypes.c_void_p * 9)]
 
 
+class TubesC(ctypes.Structure):
+    _fields_ = [("ntubes", ctypes.c_int32), ("ng", ctypes.c_int32),
+                ("ncells", ctypes.c_void_p), ("cell_off", ctypes.c_void_p),
+                ("dx", ctypes.c_void_p), ("order", ctypes.c_void_p),
+                ("cfl", ctypes.c_double), ("tend", ctypes.c_double),
+                ("max_steps", ctypes.c_int32), ("limiter", ctypes.c_int32),
+                ("solver", ctypes.c_int32), ("scheme", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("gamma", ctypes.c_double),
+                ("atmo_rho", ctypes.c_double)]
+
+
 # exported symbol -> (restype, argtypes)
 _VP = ctypes.c_void_p
 _PP = ctypes.POINTER(ctypes.c_void_p)
@@ -78,6 +89,8 @@ SIGNATURES = {
     "hlld_ct_update2d": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC), _PP,
                                         _PP, _VP, _PP, _VP, _VP, _VP, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_double, _VP, _VP]),
+    "hlld_tubes_run": (ctypes.c_int, [ctypes.POINTER(TubesC), _PP, _PP, _PP, _PP, _VP, _VP, _VP,
+                                      ctypes.c_int, ctypes.c_int, _VP]),
     "hlld_compute_dt_2d": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
                                           ctypes.c_double, _VP, _VP, _VP]),
 }

@@ -27,6 +27,7 @@ UNITS = [
     ("capi.cu", []),
     ("variant_fp64.cu", []),
     ("variant_exact.cu", ["-fmad=false"]),
+    ("variant_mixed.cu", ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("noalloc.cu", []),
 ]
 

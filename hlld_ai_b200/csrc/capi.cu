@@ -29,6 +29,11 @@ bool fp64_precision(int precision) {
     return precision == HLLD_FP64 || precision == HLLD_FP64_EXACT;
 }
 
+bool step_precision(int precision) { return fp64_precision(precision) || precision == HLLD_MIXED; }
+
+// bytes of one element of the step's primitive, flux and EMF arrays
+size_t real_bytes(int precision) { return precision == HLLD_MIXED ? 4 : 8; }
+
 int check_grid(const hlld_grid2d_t *g) {
     if (!g) return fail(HLLD_ERR_INVALID, "grid is NULL");
     if (g->nx < 1 || g->ny < 1) return fail(HLLD_ERR_INVALID, "nx, ny must be >= 1");
@@ -48,7 +53,7 @@ int check_grid(const hlld_grid2d_t *g) {
         return fail(HLLD_ERR_INVALID, "solver must be HLLE or HLLD");
     if (!(g->gamma > 1.0)) return fail(HLLD_ERR_INVALID, "gamma must be > 1");
     if (!(g->dx > 0.0) || !(g->dy > 0.0)) return fail(HLLD_ERR_INVALID, "dx, dy must be > 0");
-    if (!fp64_precision(g->precision))
+    if (!step_precision(g->precision))
         return fail(HLLD_ERR_UNSUPPORTED, "precision %d not available for the 2D step", g->precision);
     return HLLD_OK;
 }
@@ -71,19 +76,20 @@ size_t layout_scratch(const hlld_grid2d_t *g, char *base, hlld::Scratch2D *sc) {
     const size_t nxt = g->nx + 2 * g->ng, nyt = g->ny + 2 * g->ng;
     const size_t nfx = (nxt + 1) * nyt, nfy = nxt * (nyt + 1), ncr = (nxt + 1) * (nyt + 1),
                  nc = nxt * nyt;
+    const size_t rb = real_bytes(g->precision);
     size_t off = 0;
-    auto take = [&](size_t count) -> double * {
-        double *p = base ? (double *)(base + off) : nullptr;
-        off += align_up(count * sizeof(double));
+    auto take = [&](size_t count, size_t elem) -> void * {
+        void *p = base ? (void *)(base + off) : nullptr;
+        off += align_up(count * elem);
         return p;
     };
     hlld::Scratch2D s{};
-    for (int k = 0; k < 7; ++k) s.Fx[k] = take(nfx);
-    for (int k = 0; k < 7; ++k) s.Fy[k] = take(nfy);
-    s.Ez = take(ncr);
-    for (int k = 0; k < 6; ++k) s.U0[k] = take(nc);
-    s.Bx0 = take(nfx);
-    s.By0 = take(nfy);
+    for (int k = 0; k < 7; ++k) s.Fx[k] = take(nfx, rb);
+    for (int k = 0; k < 7; ++k) s.Fy[k] = take(nfy, rb);
+    s.Ez = take(ncr, rb);
+    for (int k = 0; k < 6; ++k) s.U0[k] = (double *)take(nc, 8);
+    s.Bx0 = (double *)take(nfx, 8);
+    s.By0 = (double *)take(nfy, 8);
     s.diag = base ? (hlld_step_diag_t *)(base + off) : nullptr;
     off += align_up(sizeof(hlld_step_diag_t));
     if (sc) *sc = s;
@@ -192,6 +198,8 @@ int hlld_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scrat
     cudaStream_t st = (cudaStream_t)stream;
     if (g->precision == HLLD_FP64_EXACT)
         hlld::v_exact::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
+    else if (g->precision == HLLD_MIXED)
+        hlld::v_mixed::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
     else
         hlld::v_fp64::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
     return check_launch("rk_step_ct");
@@ -207,6 +215,8 @@ int hlld_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *st
         return check_launch("sync_state diag reset");
     if (g->precision == HLLD_FP64_EXACT)
         hlld::v_exact::launch_sync_state(g, s, status, diag, st);
+    else if (g->precision == HLLD_MIXED)
+        hlld::v_mixed::launch_sync_state(g, s, status, diag, st);
     else
         hlld::v_fp64::launch_sync_state(g, s, status, diag, st);
     return check_launch("sync_state");
@@ -225,9 +235,11 @@ int hlld_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void
     if (cudaMemsetAsync(diag, 0, sizeof(hlld_flux_diag_t), st) != cudaSuccess)
         return check_launch("sweep2d diag reset");
     if (g->precision == HLLD_FP64_EXACT)
-        hlld::v_exact::launch_sweep2d(g, s, axis, (double *const *)F, diag, st);
+        hlld::v_exact::launch_sweep2d(g, s, axis, F, diag, st);
+    else if (g->precision == HLLD_MIXED)
+        hlld::v_mixed::launch_sweep2d(g, s, axis, F, diag, st);
     else
-        hlld::v_fp64::launch_sweep2d(g, s, axis, (double *const *)F, diag, st);
+        hlld::v_fp64::launch_sweep2d(g, s, axis, F, diag, st);
     return check_launch("sweep2d");
 }
 
@@ -244,23 +256,67 @@ int hlld_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *cons
         return fail(HLLD_ERR_INVALID, "NULL array argument");
     hlld::Scratch2D sc{};
     for (int k = 0; k < 7; ++k) {
-        sc.Fx[k] = (double *)Fx[k];
-        sc.Fy[k] = (double *)Fy[k];
+        sc.Fx[k] = Fx[k];
+        sc.Fy[k] = Fy[k];
         if (!sc.Fx[k] || !sc.Fy[k]) return fail(HLLD_ERR_INVALID, "flux array %d is NULL", k);
     }
     for (int k = 0; k < 6; ++k) {
         sc.U0[k] = (double *)U0[k];
         if (!sc.U0[k]) return fail(HLLD_ERR_INVALID, "U0[%d] is NULL", k);
     }
-    sc.Ez = (double *)Ez;
+    sc.Ez = Ez;
     sc.Bx0 = (double *)Bx0;
     sc.By0 = (double *)By0;
     cudaStream_t st = (cudaStream_t)stream;
     if (g->precision == HLLD_FP64_EXACT)
         hlld::v_exact::launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
+    else if (g->precision == HLLD_MIXED)
+        hlld::v_mixed::launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
     else
         hlld::v_fp64::launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
     return check_launch("ct_update2d");
+}
+
+int hlld_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
+                   void *const *U0, void *const *F, double *t_out, int32_t *steps_out,
+                   unsigned int *next, int threads, int blocks, void *stream) {
+    if (!b) return fail(HLLD_ERR_INVALID, "batch is NULL");
+    if (b->ntubes < 0) return fail(HLLD_ERR_INVALID, "ntubes < 0");
+    if (b->ntubes == 0) return HLLD_OK;
+    if (!b->ncells || !b->cell_off || !b->dx || !cons || !prims || !U0 || !F || !t_out ||
+        !steps_out || !next)
+        return fail(HLLD_ERR_INVALID, "NULL array argument");
+    if (b->limiter < 0 || b->limiter > HLLD_LIM_MP7) return fail(HLLD_ERR_INVALID, "bad limiter");
+    static const int need[6] = {1, 1, 1, 2, 2, 3};
+    if (b->ng < need[b->limiter]) return fail(HLLD_ERR_INVALID, "ng too narrow for the limiter");
+    if (b->solver != HLLD_SOLVER_HLLE && b->solver != HLLD_SOLVER_HLLD)
+        return fail(HLLD_ERR_INVALID, "solver must be HLLE or HLLD");
+    if (b->scheme != 2 && b->scheme != 3) return fail(HLLD_ERR_INVALID, "scheme must be 2 or 3");
+    if (!(b->gamma > 1.0) || !(b->cfl > 0.0)) return fail(HLLD_ERR_INVALID, "gamma, cfl");
+    if (!step_precision(b->precision)) return fail(HLLD_ERR_UNSUPPORTED, "precision %d", b->precision);
+    for (int k = 0; k < 8; ++k)
+        if (!cons[k] || !U0[k] || (k != 5 && !F[k]))
+            return fail(HLLD_ERR_INVALID, "NULL work array %d", k);
+    for (int k = 0; k < 9; ++k)
+        if (!prims[k]) return fail(HLLD_ERR_INVALID, "prims[%d] is NULL", k);
+    if (threads <= 0) threads = 256;
+    if (threads % 32 || threads > 256)
+        return fail(HLLD_ERR_INVALID, "threads must be a multiple of 32, at most 256");
+    if (blocks <= 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        blocks = sms * (256 / threads) * 2;
+    }
+    if (blocks > b->ntubes) blocks = b->ntubes;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (b->precision == HLLD_FP64_EXACT)
+        hlld::v_exact::launch_tubes_run(b, cons, prims, U0, F, t_out, steps_out, next, threads, blocks, st);
+    else if (b->precision == HLLD_MIXED)
+        hlld::v_mixed::launch_tubes_run(b, cons, prims, U0, F, t_out, steps_out, next, threads, blocks, st);
+    else
+        hlld::v_fp64::launch_tubes_run(b, cons, prims, U0, F, t_out, steps_out, next, threads, blocks, st);
+    return check_launch("tubes_run");
 }
 
 int hlld_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,
@@ -273,6 +329,8 @@ int hlld_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double c
     cudaStream_t st = (cudaStream_t)stream;
     if (g->precision == HLLD_FP64_EXACT)
         hlld::v_exact::launch_compute_dt_2d(g, s, cfl, dt_dev, work, st);
+    else if (g->precision == HLLD_MIXED)
+        hlld::v_mixed::launch_compute_dt_2d(g, s, cfl, dt_dev, work, st);
     else
         hlld::v_fp64::launch_compute_dt_2d(g, s, cfl, dt_dev, work, st);
     return check_launch("compute_dt_2d");

@@ -24,14 +24,27 @@
 #include "srmhd_phys.cuh"
 #include "variants.h"
 
+// Real type of the 2D step's primitives, reconstruction, face fluxes, corner
+// EMF and flux divergence (double, or float for the mixed form), and of the
+// HLL-state C2P that seeds the HLLD p* bracket.  The p* iteration, the cell
+// C2P and the RK accumulation of the conserved state are always double.
+#ifndef HLLD_REAL
+#define HLLD_REAL double
+#endif
+#ifndef HLLD_BRACKET_REAL
+#define HLLD_BRACKET_REAL HLLD_REAL
+#endif
+
 namespace hlld {
 namespace HLLD_NS {
 
+using R = HLLD_REAL;
+using RB = HLLD_BRACKET_REAL;
 constexpr int kThreads = 128;
 // minimum resident blocks per SM requested for the sweep kernel (caps its
 // registers at 65536 / (kThreads * this))
 #ifndef HLLD_SWEEP_MIN_BLOCKS
-#define HLLD_SWEEP_MIN_BLOCKS 1
+#define HLLD_SWEEP_MIN_BLOCKS 4
 #endif
 
 // ── small utilities ──────────────────────────────────────────────────────
@@ -306,8 +319,9 @@ enum { F_D = 0, F_SX, F_SY, F_SZ, F_TAU, F_BZ, F_BT, NFLUX };
 
 struct SweepParams {
     Grid g;
-    const double *rho, *p, *vx, *vy, *vz, *bz, *Bxf, *Byf;
-    double *F[NFLUX];
+    const R *rho, *p, *vx, *vy, *vz, *bz;
+    const double *Bxf, *Byf;
+    R *F[NFLUX];
     hlld_flux_diag_t *diag;
 };
 
@@ -315,7 +329,7 @@ struct SweepParams {
 // the lower-x face of cell (f, j).  AXIS 1: faces (nxt, nyt+1).
 template <int AXIS, int LIM, int SOLVER>
 __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(const SweepParams p) {
-    using T = double;
+    using T = R;
     constexpr int S = Stencil<LIM>::S;
     constexpr int NW = 2 * S + 2;
     const Grid &g = p.g;
@@ -331,9 +345,15 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         const int n = AXIS == 0 ? g.nxt : g.nyt;
         const int64_t cstride = AXIS == 0 ? g.nyt : 1;
         const int64_t cbase = AXIS == 0 ? (int64_t)tr : (int64_t)tr * g.nyt;
+        // transverse in-plane B at cell c, averaged from its faces (ct.py:44-54)
+        auto bt_at = [&](int c) -> T {
+            return AXIS == 0
+                       ? T(0.5 * (p.Byf[(int64_t)c * (g.nyt + 1) + tr] + p.Byf[(int64_t)c * (g.nyt + 1) + tr + 1]))
+                       : T(0.5 * (p.Bxf[(int64_t)tr * g.nyt + c] + p.Bxf[(int64_t)(tr + 1) * g.nyt + c]));
+        };
         // work variables (reconstruction.py:269): rho, p, W vx, W vy, W vz,
-        // transverse in-plane B (cell-centred from faces, ct.py:44-54), Bz
-        T L[7], R[7];
+        // transverse in-plane B, Bz
+        T L[7], Rt[7];
         if (f == 0 || f == n) {
             // outermost faces: the edge cell has zero slope in every scheme
             const int c = f == 0 ? 0 : n - 1;
@@ -341,13 +361,11 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
             T vx = p.vx[ci], vy = p.vy[ci], vz = p.vz[ci];
             T v2 = vx * vx + vy * vy + vz * vz;
             T W = T(1) / sqrt(clamp_lo(T(1) - v2, T(1e-14)));
-            T bt = AXIS == 0 ? T(0.5) * (p.Byf[(int64_t)c * (g.nyt + 1) + tr] + p.Byf[(int64_t)c * (g.nyt + 1) + tr + 1])
-                             : T(0.5) * (p.Bxf[(int64_t)tr * g.nyt + c] + p.Bxf[(int64_t)(tr + 1) * g.nyt + c]);
-            T q[7] = {p.rho[ci], p.p[ci], W * vx, W * vy, W * vz, bt, p.bz[ci]};
+            T q[7] = {p.rho[ci], p.p[ci], W * vx, W * vy, W * vz, bt_at(c), p.bz[ci]};
 #pragma unroll
             for (int k = 0; k < 7; ++k) {
                 L[k] = q[k] + T(0.5) * T(0);
-                R[k] = q[k] - T(0.5) * T(0);
+                Rt[k] = q[k] - T(0.5) * T(0);
             }
         } else {
             // window of cells f-1-S .. f+S (clamped; clamped entries are never
@@ -381,39 +399,36 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
                     case 2: x = Wf[k] * p.vx[ci]; break;
                     case 3: x = Wf[k] * p.vy[ci]; break;
                     case 4: x = Wf[k] * p.vz[ci]; break;
-                    case 5:
-                        x = AXIS == 0 ? T(0.5) * (p.Byf[(int64_t)c * (g.nyt + 1) + tr] + p.Byf[(int64_t)c * (g.nyt + 1) + tr + 1])
-                                      : T(0.5) * (p.Bxf[(int64_t)tr * g.nyt + c] + p.Bxf[(int64_t)(tr + 1) * g.nyt + c]);
-                        break;
+                    case 5: x = bt_at(c); break;
                     default: x = p.bz[ci]; break;
                     }
                     w[k] = x;
                 }
                 L[v] = cell_edge<LIM, true, S>(w, f - 1, n);
-                R[v] = cell_edge<LIM, false, S + 1>(w, f, n);
+                Rt[v] = cell_edge<LIM, false, S + 1>(w, f, n);
                 pcmL[v] = w[S];
                 pcmR[v] = w[S + 1];
             }
             if (LIM != HLLD_LIM_PCM) {
                 // positivity fallback to PCM (reconstruction.py:315-326)
-                bool bad = (L[0] <= T(1e-12)) || (R[0] <= T(1e-12)) || (L[1] <= T(1e-14)) ||
-                           (R[1] <= T(1e-14));
+                bool bad = (L[0] <= T(1e-12)) || (Rt[0] <= T(1e-12)) || (L[1] <= T(1e-14)) ||
+                           (Rt[1] <= T(1e-14));
                 if (bad) {
 #pragma unroll
                     for (int v = 0; v < 7; ++v) {
                         L[v] = pcmL[v] + T(0.5) * T(0);
-                        R[v] = pcmR[v] - T(0.5) * T(0);
+                        Rt[v] = pcmR[v] - T(0.5) * T(0);
                     }
                 }
             }
         }
         // Wv -> v, floors, EOS-consistent eps (reconstruction.py:328-336); the
         // normal field is the face value (sweep.py:82-89)
-        const T bn = AXIS == 0 ? p.Bxf[(int64_t)f * g.nyt + tr] : p.Byf[(int64_t)tr * (g.nyt + 1) + f];
+        const T bn = T(AXIS == 0 ? p.Bxf[(int64_t)f * g.nyt + tr] : p.Byf[(int64_t)tr * (g.nyt + 1) + f]);
         T PL[NPRIM], PR[NPRIM];
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
-            T *q = side == 0 ? L : R;
+            T *q = side == 0 ? L : Rt;
             T *P = side == 0 ? PL : PR;
             T z2 = q[2] * q[2] + q[3] * q[3] + q[4] * q[4];
             T fac = T(1) / sqrt(T(1) + z2);
@@ -429,7 +444,7 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         }
         FaceOut<T> o;
         if (SOLVER == HLLD_SOLVER_HLLD)
-            hlld_face<AXIS, T>(PL, PR, (T)g.gamma, false, o);
+            hlld_face<AXIS, T, RB, double>(PL, PR, (T)g.gamma, false, o);
         else
             hlle_face<AXIS, T>(PL, PR, (T)g.gamma, false, false, o);
         const int64_t fi = e;
@@ -449,65 +464,67 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         cnt.v[6] = o.err == 0;
         cnt.v[7] = (unsigned long long)o.iters;
         // max |F_D| over the sweep, for the CT deadband (ct.py:114)
-        cnt.v[8] = abs_bits(o.F[C_D]);
+        cnt.v[8] = abs_bits((double)o.F[C_D]);
     }
     unsigned long long *mx[2] = {&p.diag->max_iters, &p.diag->fd_max_bits};
     block_accumulate<7, 2>(cnt, &p.diag->n_faces, mx);
 }
 
 // ct.py:96-116 with the sweep-global scale
-__device__ __forceinline__ double upwind_sign(double F, double scale) {
-    return (fabs(F) > 1e-9 * scale) ? tsign(F) : 0.0;
+template <typename T> __device__ __forceinline__ T upwind_sign(T F, T scale) {
+    return (fabs(F) > T(1e-9) * scale) ? tsign(F) : T(0);
 }
 
 struct CtParams {
     Grid g;
-    const double *vx, *vy, *Bxf, *Byf;
-    const double *FxD, *FyD, *FxBt, *FyBt;
+    const R *vx, *vy;
+    const double *Bxf, *Byf;
+    const R *FxD, *FyD, *FxBt, *FyBt;
     const hlld_step_diag_t *diag;
     int upwind;
-    double *Ez;
+    R *Ez;
 };
 
 // cell-centred E^z = v^y B^x - v^x B^y from face-averaged B (ct.py:44-60)
-__device__ __forceinline__ double cell_emf(const CtParams &p, int i, int j) {
+__device__ __forceinline__ R cell_emf(const CtParams &p, int i, int j) {
     const int nyt = p.g.nyt;
-    double Bcx = 0.5 * (p.Bxf[(int64_t)i * nyt + j] + p.Bxf[(int64_t)(i + 1) * nyt + j]);
-    double Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
+    R Bcx = R(0.5 * (p.Bxf[(int64_t)i * nyt + j] + p.Bxf[(int64_t)(i + 1) * nyt + j]));
+    R Bcy = R(0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]));
     int64_t c = (int64_t)i * nyt + j;
     return Bcx * p.vy[c] - Bcy * p.vx[c];
 }
 
 __global__ void __launch_bounds__(kThreads) ct_emf_kernel(const CtParams p) {
+    using T = R;
     const int nxt = p.g.nxt, nyt = p.g.nyt;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (int64_t)(nxt + 1) * (nyt + 1)) return;
     const int i = (int)(e / (nyt + 1)), j = (int)(e - (int64_t)i * (nyt + 1));
-    double val = 0.0;
+    T val = T(0);
     if (i >= 1 && i <= nxt - 1 && j >= 1 && j <= nyt - 1) {
         // Efy (nxt, nyt+1) = +F^y(Bx); Efx (nxt+1, nyt) = -F^x(By)
-        double Ezyf = p.FyBt[(int64_t)i * (nyt + 1) + j];
-        double Ezyfm = p.FyBt[(int64_t)(i - 1) * (nyt + 1) + j];
-        double Ezxf = -p.FxBt[(int64_t)i * nyt + j];
-        double Ezxfm = -p.FxBt[(int64_t)i * nyt + j - 1];
-        double EzNE = cell_emf(p, i, j);
-        double EzNW = cell_emf(p, i - 1, j);
-        double EzSE = cell_emf(p, i, j - 1);
-        double EzSW = cell_emf(p, i - 1, j - 1);
-        double Eavg = 0.25 * ((Ezyf + Ezyfm) + (Ezxf + Ezxfm));
+        T Ezyf = p.FyBt[(int64_t)i * (nyt + 1) + j];
+        T Ezyfm = p.FyBt[(int64_t)(i - 1) * (nyt + 1) + j];
+        T Ezxf = -p.FxBt[(int64_t)i * nyt + j];
+        T Ezxfm = -p.FxBt[(int64_t)i * nyt + j - 1];
+        T EzNE = cell_emf(p, i, j);
+        T EzNW = cell_emf(p, i - 1, j);
+        T EzSE = cell_emf(p, i, j - 1);
+        T EzSW = cell_emf(p, i - 1, j - 1);
+        T Eavg = T(0.25) * ((Ezyf + Ezyfm) + (Ezxf + Ezxfm));
         if (p.upwind) {
-            double sx = __longlong_as_double((long long)p.diag->sweep[0].fd_max_bits);
-            double sy = __longlong_as_double((long long)p.diag->sweep[1].fd_max_bits);
-            double Sx = upwind_sign(p.FxD[(int64_t)i * nyt + j], sx);
-            double Sxm = upwind_sign(p.FxD[(int64_t)i * nyt + j - 1], sx);
-            double dEdyN = (1.0 - Sx) * (EzNE - Ezyf) + (1.0 + Sx) * (EzNW - Ezyfm);
-            double dEdyS = (1.0 - Sxm) * (Ezyf - EzSE) + (1.0 + Sxm) * (Ezyfm - EzSW);
-            double dEdy = 0.125 * (dEdyS - dEdyN);
-            double Sy = upwind_sign(p.FyD[(int64_t)i * (nyt + 1) + j], sy);
-            double Sym = upwind_sign(p.FyD[(int64_t)(i - 1) * (nyt + 1) + j], sy);
-            double dEdxE = (1.0 - Sy) * (EzNE - Ezxf) + (1.0 + Sy) * (EzSE - Ezxfm);
-            double dEdxW = (1.0 - Sym) * (Ezxf - EzNW) + (1.0 + Sym) * (Ezxfm - EzSW);
-            double dEdx = 0.125 * (dEdxW - dEdxE);
+            T sx = T(__longlong_as_double((long long)p.diag->sweep[0].fd_max_bits));
+            T sy = T(__longlong_as_double((long long)p.diag->sweep[1].fd_max_bits));
+            T Sx = upwind_sign(p.FxD[(int64_t)i * nyt + j], sx);
+            T Sxm = upwind_sign(p.FxD[(int64_t)i * nyt + j - 1], sx);
+            T dEdyN = (T(1) - Sx) * (EzNE - Ezyf) + (T(1) + Sx) * (EzNW - Ezyfm);
+            T dEdyS = (T(1) - Sxm) * (Ezyf - EzSE) + (T(1) + Sxm) * (Ezyfm - EzSW);
+            T dEdy = T(0.125) * (dEdyS - dEdyN);
+            T Sy = upwind_sign(p.FyD[(int64_t)i * (nyt + 1) + j], sy);
+            T Sym = upwind_sign(p.FyD[(int64_t)(i - 1) * (nyt + 1) + j], sy);
+            T dEdxE = (T(1) - Sy) * (EzNE - Ezxf) + (T(1) + Sy) * (EzSE - Ezxfm);
+            T dEdxW = (T(1) - Sym) * (Ezxf - EzNW) + (T(1) + Sym) * (Ezxfm - EzSW);
+            T dEdx = T(0.125) * (dEdxW - dEdxE);
             val = Eavg + (dEdy + dEdx);
         } else {
             val = Eavg;
@@ -521,17 +538,18 @@ struct UpdateParams {
     double *U[6];
     double *U0[6];
     double *Bxf, *Byf, *Bx0, *By0;
-    const double *Fx[6];
-    const double *Fy[6];
-    const double *Ez;
+    const R *Fx[6];
+    const R *Fy[6];
+    const R *Ez;
     const double *dt_dev;
     double dt_host;
     double a, b, c;
     int first_stage;
 };
 
-// flux divergence + CT face update + RK combine on the physical block and
-// its upper faces; a thread owns cell (i, j), face Bxf(i, j), face Byf(i, j)
+// flux divergence (in R) + CT face update + RK combine (in double) on the
+// physical block and its upper faces; a thread owns cell (i, j), face
+// Bxf(i, j) and face Byf(i, j)
 __global__ void __launch_bounds__(kThreads) ct_update_kernel(const UpdateParams p) {
     const Grid &g = p.g;
     const int nyt = g.nyt;
@@ -541,13 +559,14 @@ __global__ void __launch_bounds__(kThreads) ct_update_kernel(const UpdateParams 
     const int i = g.ng + ii, j = g.ng + jj;
     const double dt = p.dt_dev ? *p.dt_dev : p.dt_host;
     const double w2 = p.c * dt;
+    const R rdx = R(g.dx), rdy = R(g.dy);
     if (ii < g.nx && jj < g.ny) {
         const int64_t c = (int64_t)i * nyt + j;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            double rx = -(p.Fx[k][(int64_t)(i + 1) * nyt + j] - p.Fx[k][c]) / g.dx;
-            double ry = -(p.Fy[k][(int64_t)i * (nyt + 1) + j + 1] - p.Fy[k][(int64_t)i * (nyt + 1) + j]) / g.dy;
-            double L = rx + ry;
+            R rx = -(p.Fx[k][(int64_t)(i + 1) * nyt + j] - p.Fx[k][c]) / rdx;
+            R ry = -(p.Fy[k][(int64_t)i * (nyt + 1) + j + 1] - p.Fy[k][(int64_t)i * (nyt + 1) + j]) / rdy;
+            double L = (double)(rx + ry);
             double u = p.U[k][c];
             double u0;
             if (p.first_stage) {
@@ -564,7 +583,7 @@ __global__ void __launch_bounds__(kThreads) ct_update_kernel(const UpdateParams 
     }
     if (jj < g.ny) {
         const int64_t fx = (int64_t)i * nyt + j;
-        double dB = (p.Ez[(int64_t)i * (nyt + 1) + j] - p.Ez[(int64_t)i * (nyt + 1) + j + 1]) / g.dy;
+        double dB = ((double)p.Ez[(int64_t)i * (nyt + 1) + j] - (double)p.Ez[(int64_t)i * (nyt + 1) + j + 1]) / g.dy;
         double u = p.Bxf[fx];
         double u0;
         if (p.first_stage) {
@@ -580,7 +599,7 @@ __global__ void __launch_bounds__(kThreads) ct_update_kernel(const UpdateParams 
     }
     if (ii < g.nx) {
         const int64_t fy = (int64_t)i * (nyt + 1) + j;
-        double dB = (p.Ez[(int64_t)(i + 1) * (nyt + 1) + j] - p.Ez[(int64_t)i * (nyt + 1) + j]) / g.dx;
+        double dB = ((double)p.Ez[(int64_t)(i + 1) * (nyt + 1) + j] - (double)p.Ez[(int64_t)i * (nyt + 1) + j]) / g.dx;
         double u = p.Byf[fy];
         double u0;
         if (p.first_stage) {
@@ -617,8 +636,8 @@ __device__ __forceinline__ int bc_face_src(int idx, int n, int ng, int kind) {
     return idx;
 }
 
-struct GhostParams {
-    double *v[9];  // blockIdx.y selects the array
+template <typename E> struct GhostParams {
+    E *v[9];       // blockIdx.y selects the array
     int n0, n1;    // array shape
     int a0, b0, a1, b1;  // block never written (its entries are every source)
     int n_ph0, n_ph1, ng;
@@ -628,8 +647,9 @@ struct GhostParams {
 
 // Fills every entry outside [a0,b0) x [a1,b1) from its separable source;
 // all sources lie inside that block, so the fill is race free in place.
-__global__ void __launch_bounds__(kThreads) ghost_kernel(const GhostParams p) {
-    double *v = p.v[blockIdx.y];
+template <typename E>
+__global__ void __launch_bounds__(kThreads) ghost_kernel(const GhostParams<E> p) {
+    E *v = p.v[blockIdx.y];
     const int in0 = p.b0 - p.a0, in1 = p.b1 - p.a1;
     const int64_t nA = (int64_t)(p.n0 - in0) * p.n1;
     const int64_t nB = (int64_t)in0 * (p.n1 - in1);
@@ -657,12 +677,13 @@ struct C2PCellsParams {
     Grid g;
     const double *U[6];
     const double *Bxf, *Byf;
-    double *P[9];
+    R *P[9];
     uint8_t *status;
     hlld_step_diag_t *diag;
 };
 
-// cell-centred B (ct.py:44-54) + C2P (c2p.py:313-363) of the physical cells
+// cell-centred B (ct.py:44-54) + C2P (c2p.py:313-363) of the physical cells,
+// in double; primitives stored as R
 __global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParams p) {
     const Grid &g = p.g;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -677,7 +698,7 @@ __global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParam
         double P[NPRIM];
         uint8_t st = cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P);
 #pragma unroll
-        for (int k = 0; k < NPRIM; ++k) p.P[k][c] = P[k];
+        for (int k = 0; k < NPRIM; ++k) p.P[k][c] = (R)P[k];
         if (p.status) p.status[c] = st;
         cnt.v[0] = !(st & ST_CONVERGED);
         cnt.v[1] = (st & ST_BISECTED) != 0;
@@ -689,11 +710,11 @@ __global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParam
 
 struct SpeedParams {
     Grid g;
-    const double *P[9];
+    const R *P[9];
     unsigned long long *out;  // [2]
 };
 
-// max(|v_d| + c_f) over the physical cells (driver2d.py:260-279)
+// max(|v_d| + c_f) over the physical cells (driver2d.py:260-279), in double
 __global__ void __launch_bounds__(kThreads) speed_kernel(const SpeedParams p) {
     const Grid &g = p.g;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -737,6 +758,261 @@ __global__ void dt_kernel(const unsigned long long *speeds, double dx, double dy
     }
     double sx = clamp_lo(mx, 1e-14), sy = clamp_lo(my, 1e-14);
     *dt = (1.0 / (sx / dx + sy / dy)) * cfl;
+}
+
+// driver2d.py:104-105 in device memory
+__constant__ double kRK3d[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
+__constant__ double kRK2d[2][3] = {{1.0, 0.0, 1.0}, {0.5, 0.5, 0.5}};
+
+// ── batched 1D tubes (one persistent launch) ─────────────────────────────
+//
+// Each tube is driver2d.py:309-355 rk_step on a ny = 1 grid (whose y sweep
+// contributes exactly zero), advanced to tend with its own dt
+// (driver.py:77-127 compute_dt).  A CTA takes whole tubes from an atomic
+// counter (in the caller's order, e.g. longest first) and time-steps each
+// one with block barriers between the face, update, boundary and C2P
+// phases; a tube's arrays live in the concatenated cell / face arrays.
+
+struct TubesParams {
+    int ntubes, ng, max_steps, scheme;
+    const int32_t *ncells;
+    const int64_t *cell_off;  // first cell (ghosts included) of each tube
+    const double *dx;
+    const int32_t *order;
+    double cfl, tend, gamma, atmo_rho;
+    double *U[8];   // conserved, all eight components
+    double *U0[8];
+    R *P[9];        // primitives
+    R *F[8];        // face fluxes (slot C_BX unused: F[Bx] = 0)
+    double *t_out;
+    int32_t *steps_out;
+    unsigned int *next;
+};
+
+template <int LIM, int SOLVER>
+__device__ __forceinline__ void tube_face(const TubesParams &p, int64_t base, int nt, int f,
+                                          int64_t fout) {
+    using T = R;
+    constexpr int S = Stencil<LIM>::S;
+    constexpr int NW = 2 * S + 2;
+    // work variables (reconstruction.py:269) with vel_var Wv, all eight
+    // (no face-B override: sweep.py Bnf = None)
+    T L[8], Rt[8];
+    if (f == 0 || f == nt) {
+        const int64_t ci = base + (f == 0 ? 0 : nt - 1);
+        T vx = p.P[P_VX][ci], vy = p.P[P_VY][ci], vz = p.P[P_VZ][ci];
+        T v2 = vx * vx + vy * vy + vz * vz;
+        T W = T(1) / sqrt(clamp_lo(T(1) - v2, T(1e-14)));
+        T q[8] = {p.P[P_RHO][ci], p.P[P_P][ci], W * vx, W * vy, W * vz,
+                  p.P[P_BX][ci], p.P[P_BY][ci], p.P[P_BZ][ci]};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            L[k] = q[k] + T(0.5) * T(0);
+            Rt[k] = q[k] - T(0.5) * T(0);
+        }
+    } else {
+        int cw[NW];
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            int c = f - 1 - S + k;
+            cw[k] = c < 0 ? 0 : (c > nt - 1 ? nt - 1 : c);
+        }
+        T Wf[NW];
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            const int64_t ci = base + cw[k];
+            T vx = p.P[P_VX][ci], vy = p.P[P_VY][ci], vz = p.P[P_VZ][ci];
+            T v2 = vx * vx + vy * vy + vz * vz;
+            Wf[k] = T(1) / sqrt(clamp_lo(T(1) - v2, T(1e-14)));
+        }
+        T pcmL[8], pcmR[8];
+        constexpr int src[8] = {P_RHO, P_P, P_VX, P_VY, P_VZ, P_BX, P_BY, P_BZ};
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+            T w[NW];
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                T x = p.P[src[v]][base + cw[k]];
+                w[k] = (v >= 2 && v <= 4) ? Wf[k] * x : x;
+            }
+            L[v] = cell_edge<LIM, true, S>(w, f - 1, nt);
+            Rt[v] = cell_edge<LIM, false, S + 1>(w, f, nt);
+            pcmL[v] = w[S];
+            pcmR[v] = w[S + 1];
+        }
+        if (LIM != HLLD_LIM_PCM) {
+            bool bad = (L[0] <= T(1e-12)) || (Rt[0] <= T(1e-12)) || (L[1] <= T(1e-14)) ||
+                       (Rt[1] <= T(1e-14));
+            if (bad) {
+#pragma unroll
+                for (int v = 0; v < 8; ++v) {
+                    L[v] = pcmL[v] + T(0.5) * T(0);
+                    Rt[v] = pcmR[v] - T(0.5) * T(0);
+                }
+            }
+        }
+    }
+    T PL[NPRIM], PR[NPRIM];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        T *q = side == 0 ? L : Rt;
+        T *P = side == 0 ? PL : PR;
+        T z2 = q[2] * q[2] + q[3] * q[3] + q[4] * q[4];
+        T fac = T(1) / sqrt(T(1) + z2);
+        P[P_VX] = q[2] * fac;
+        P[P_VY] = q[3] * fac;
+        P[P_VZ] = q[4] * fac;
+        P[P_RHO] = clamp_lo(q[0], T(1e-12));
+        P[P_P] = clamp_lo(q[1], T(1e-14));
+        P[P_EPS] = eos_eps(P[P_P], P[P_RHO], (T)p.gamma);
+        P[P_BX] = q[5];
+        P[P_BY] = q[6];
+        P[P_BZ] = q[7];
+    }
+    FaceOut<T> o;
+    if (SOLVER == HLLD_SOLVER_HLLD)
+        hlld_face<0, T, RB, double>(PL, PR, (T)p.gamma, false, o);
+    else
+        hlle_face<0, T>(PL, PR, (T)p.gamma, false, false, o);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        if (k != C_BX) p.F[k][fout] = o.F[k];
+}
+
+__device__ __forceinline__ unsigned long long block_max_any(unsigned long long x,
+                                                            unsigned long long *sm) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long y = __shfl_down_sync(0xffffffffu, x, o);
+        x = x > y ? x : y;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm[w] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long r = sm[0];
+        for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) r = r > sm[ww] ? r : sm[ww];
+        sm[32] = r;
+    }
+    __syncthreads();
+    unsigned long long r = sm[32];
+    __syncthreads();
+    return r;
+}
+
+template <int LIM, int SOLVER>
+__global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
+    __shared__ unsigned long long red[33];
+    __shared__ int s_tube;
+    const int ng = p.ng;
+    for (;;) {
+        if (threadIdx.x == 0) s_tube = (int)atomicAdd(p.next, 1u);
+        __syncthreads();
+        const int q = s_tube;
+        __syncthreads();
+        if (q >= p.ntubes) return;
+        const int ti = p.order ? p.order[q] : q;
+        const int L = p.ncells[ti];
+        const int nt = L + 2 * ng;
+        const int64_t base = p.cell_off[ti];
+        const int64_t fbase = base + ti;  // tube ti has nt + 1 faces
+        const double dx = p.dx[ti];
+        // conserved variables from the primitives (hlld.py:185-217)
+        for (int c = threadIdx.x; c < nt; c += blockDim.x) {
+            double Pd[NPRIM], Cd[NCONS];
+#pragma unroll
+            for (int k = 0; k < NPRIM; ++k) Pd[k] = (double)p.P[k][base + c];
+            prim_to_cons<double>(Pd, Cd);
+#pragma unroll
+            for (int k = 0; k < NCONS; ++k) p.U[k][base + c] = Cd[k];
+        }
+        __syncthreads();
+        double t = 0.0;
+        int steps = 0;
+        const int nst = p.scheme == 3 ? 3 : 2;
+        while (t < p.tend - 1e-14 && steps < p.max_steps) {
+            // dt = (cfl dx) / max(|vx| + v_fast) over the physical cells
+            unsigned long long mloc = 0;
+            for (int c = ng + threadIdx.x; c < ng + L; c += blockDim.x) {
+                const int64_t ci = base + c;
+                double rho = p.P[P_RHO][ci], eps = p.P[P_EPS][ci];
+                double vx = p.P[P_VX][ci], vy = p.P[P_VY][ci], vz = p.P[P_VZ][ci];
+                double Bx = p.P[P_BX][ci], By = p.P[P_BY][ci], Bz = p.P[P_BZ][ci];
+                double pr, cs2;
+                eos_press_cs2(eps, rho, p.gamma, pr, cs2);
+                double v2 = vx * vx + vy * vy + vz * vz;
+                double W = 1.0 / sqrt(clamp_lo(1.0 - v2, 1e-10));
+                double B2 = Bx * Bx + By * By + Bz * Bz;
+                double vdotB = vx * Bx + vy * By + vz * Bz;
+                double b2 = (B2 + vdotB * vdotB) / (W * W);
+                double h = 1.0 + eps + pr / rho;
+                double v02 = cs2 + (b2 / (rho * h + b2)) * (1.0 - cs2);
+                double vf = sqrt(clamp_hi(clamp_lo(v02, 0.0), 1.0));
+                unsigned long long b = abs_bits(fabs(vx) + vf);
+                mloc = mloc > b ? mloc : b;
+            }
+            const double mx = __longlong_as_double((long long)block_max_any(mloc, red));
+            double dt = isnan(mx) ? mx : (1.0 / clamp_lo(mx, 1e-14)) * (p.cfl * dx);
+            if (dt > p.tend - t) dt = p.tend - t;
+            if (!(dt > 0.0)) break;
+            for (int c = threadIdx.x; c < nt; c += blockDim.x)
+#pragma unroll
+                for (int k = 0; k < 8; ++k) p.U0[k][base + c] = p.U[k][base + c];
+            for (int st = 0; st < nst; ++st) {
+                const double *w = p.scheme == 3 ? kRK3d[st] : kRK2d[st];
+                const double w2 = w[2] * dt;
+                for (int f = threadIdx.x; f <= nt; f += blockDim.x)
+                    tube_face<LIM, SOLVER>(p, base, nt, f, fbase + f);
+                __syncthreads();
+                for (int c = threadIdx.x; c < nt; c += blockDim.x) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        double rhs;
+                        if (k == C_BX) {
+                            rhs = -(0.0 - 0.0) / dx + (-0.0);
+                        } else {
+                            R d = p.F[k][fbase + c + 1] - p.F[k][fbase + c];
+                            rhs = (double)(-d / R(dx)) + (-0.0);
+                        }
+                        double v = w[0] * p.U0[k][base + c] + w[1] * p.U[k][base + c];
+                        p.U[k][base + c] = v + w2 * rhs;
+                    }
+                }
+                __syncthreads();
+                // outflow BCs on the conserved variables (grid.py:93-113)
+                for (int c = threadIdx.x; c < 2 * ng; c += blockDim.x) {
+                    const int gc = c < ng ? c : L + c;
+                    const int sc = c < ng ? ng : ng + L - 1;
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) p.U[k][base + gc] = p.U[k][base + sc];
+                }
+                __syncthreads();
+                for (int c = ng + threadIdx.x; c < ng + L; c += blockDim.x) {
+                    double Cd[NCONS], Pd[NPRIM];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) Cd[k] = p.U[k][base + c];
+                    cons_to_prim<double>(Cd, p.gamma, p.atmo_rho, 1e-10, Pd);
+#pragma unroll
+                    for (int k = 0; k < NPRIM; ++k) p.P[k][base + c] = (R)Pd[k];
+                }
+                __syncthreads();
+                for (int c = threadIdx.x; c < 2 * ng; c += blockDim.x) {
+                    const int gc = c < ng ? c : L + c;
+                    const int sc = c < ng ? ng : ng + L - 1;
+#pragma unroll
+                    for (int k = 0; k < NPRIM; ++k) p.P[k][base + gc] = p.P[k][base + sc];
+                }
+                __syncthreads();
+            }
+            t += dt;
+            ++steps;
+        }
+        if (threadIdx.x == 0) {
+            p.t_out[ti] = t;
+            p.steps_out[ti] = steps;
+        }
+        __syncthreads();
+    }
 }
 
 // ── host-side launchers of this variant ──────────────────────────────────
@@ -835,8 +1111,9 @@ static void launch_sweep(int limiter, int solver, const SweepParams &sp, cudaStr
     }
 }
 
-static void launch_ghost_cc(const Grid &G, double *const *arrs, int narr, cudaStream_t st) {
-    GhostParams gp = {};
+template <typename E>
+static void launch_ghost_cc(const Grid &G, E *const *arrs, int narr, cudaStream_t st) {
+    GhostParams<E> gp = {};
     for (int k = 0; k < narr; ++k) gp.v[k] = arrs[k];
     gp.n0 = G.nxt;
     gp.n1 = G.nyt;
@@ -850,12 +1127,12 @@ static void launch_ghost_cc(const Grid &G, double *const *arrs, int narr, cudaSt
     gp.kind0 = G.bc_x;
     gp.kind1 = G.bc_y;
     int64_t cnt = (int64_t)gp.n0 * gp.n1 - (int64_t)(gp.b0 - gp.a0) * (gp.b1 - gp.a1);
-    ghost_kernel<<<dim3(grid1d(cnt), narr), kThreads, 0, st>>>(gp);
+    ghost_kernel<E><<<dim3(grid1d(cnt), narr), kThreads, 0, st>>>(gp);
 }
 
 static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStream_t st) {
     // Bxf: face rule along x, cell rule along y (grid.py:250-251)
-    GhostParams gp = {};
+    GhostParams<double> gp = {};
     gp.v[0] = Bxf;
     gp.n0 = G.nxt + 1;
     gp.n1 = G.nyt;
@@ -871,9 +1148,9 @@ static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStre
     gp.face0 = 1;
     gp.face1 = 0;
     int64_t cnt = (int64_t)gp.n0 * gp.n1 - (int64_t)(gp.b0 - gp.a0) * (gp.b1 - gp.a1);
-    ghost_kernel<<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gp);
+    ghost_kernel<double><<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gp);
     // Byf: cell rule along x, face rule along y (grid.py:253-254)
-    GhostParams gq = {};
+    GhostParams<double> gq = {};
     gq.v[0] = Byf;
     gq.n0 = G.nxt;
     gq.n1 = G.nyt + 1;
@@ -889,7 +1166,7 @@ static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStre
     gq.face0 = 0;
     gq.face1 = 1;
     cnt = (int64_t)gq.n0 * gq.n1 - (int64_t)(gq.b0 - gq.a0) * (gq.b1 - gq.a1);
-    ghost_kernel<<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gq);
+    ghost_kernel<double><<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gq);
 }
 
 void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
@@ -897,10 +1174,10 @@ void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t 
     Grid G = make_grid(g);
     double *cons[6];
     for (int k = 0; k < 6; ++k) cons[k] = (double *)s->cons[k];
-    double *prims[9];
-    for (int k = 0; k < 9; ++k) prims[k] = (double *)s->prims[k];
+    R *prims[9];
+    for (int k = 0; k < 9; ++k) prims[k] = (R *)s->prims[k];
     launch_ghost_faces(G, (double *)s->Bxf, (double *)s->Byf, st);
-    launch_ghost_cc(G, cons, 6, st);
+    launch_ghost_cc<double>(G, cons, 6, st);
     C2PCellsParams cp = {};
     cp.g = G;
     for (int k = 0; k < 6; ++k) cp.U[k] = cons[k];
@@ -910,22 +1187,22 @@ void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t 
     cp.status = status;
     cp.diag = diag;
     c2p_cells_kernel<<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(cp);
-    launch_ghost_cc(G, prims, 9, st);
+    launch_ghost_cc<R>(G, prims, 9, st);
 }
 
-void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis,
-                    double *const *F, hlld_flux_diag_t *fdiag, cudaStream_t st) {
+void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
+                    hlld_flux_diag_t *fdiag, cudaStream_t st) {
     SweepParams sp = {};
     sp.g = make_grid(g);
-    sp.rho = (const double *)s->prims[P_RHO];
-    sp.p = (const double *)s->prims[P_P];
-    sp.vx = (const double *)s->prims[P_VX];
-    sp.vy = (const double *)s->prims[P_VY];
-    sp.vz = (const double *)s->prims[P_VZ];
-    sp.bz = (const double *)s->prims[P_BZ];
+    sp.rho = (const R *)s->prims[P_RHO];
+    sp.p = (const R *)s->prims[P_P];
+    sp.vx = (const R *)s->prims[P_VX];
+    sp.vy = (const R *)s->prims[P_VY];
+    sp.vz = (const R *)s->prims[P_VZ];
+    sp.bz = (const R *)s->prims[P_BZ];
     sp.Bxf = (const double *)s->Bxf;
     sp.Byf = (const double *)s->Byf;
-    for (int k = 0; k < NFLUX; ++k) sp.F[k] = F[k];
+    for (int k = 0; k < NFLUX; ++k) sp.F[k] = (R *)F[k];
     sp.diag = fdiag;
     if (axis == 0) launch_sweep<0>(g->limiter, g->solver, sp, st);
     else launch_sweep<1>(g->limiter, g->solver, sp, st);
@@ -943,31 +1220,31 @@ void launch_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, const S
     const int64_t ncorner = (int64_t)(G.nxt + 1) * (G.nyt + 1);
     CtParams cp = {};
     cp.g = G;
-    cp.vx = (const double *)s->prims[P_VX];
-    cp.vy = (const double *)s->prims[P_VY];
+    cp.vx = (const R *)s->prims[P_VX];
+    cp.vy = (const R *)s->prims[P_VY];
     cp.Bxf = (const double *)s->Bxf;
     cp.Byf = (const double *)s->Byf;
-    cp.FxD = sc.Fx[F_D];
-    cp.FyD = sc.Fy[F_D];
-    cp.FxBt = sc.Fx[F_BT];
-    cp.FyBt = sc.Fy[F_BT];
+    cp.FxD = (const R *)sc.Fx[F_D];
+    cp.FyD = (const R *)sc.Fy[F_D];
+    cp.FxBt = (const R *)sc.Fx[F_BT];
+    cp.FyBt = (const R *)sc.Fy[F_BT];
     cp.diag = diag;
     cp.upwind = g->upwind;
-    cp.Ez = sc.Ez;
+    cp.Ez = (R *)sc.Ez;
     ct_emf_kernel<<<grid1d(ncorner), kThreads, 0, st>>>(cp);
     UpdateParams up = {};
     up.g = G;
     for (int k = 0; k < 6; ++k) {
         up.U[k] = (double *)s->cons[k];
         up.U0[k] = sc.U0[k];
-        up.Fx[k] = sc.Fx[k];
-        up.Fy[k] = sc.Fy[k];
+        up.Fx[k] = (const R *)sc.Fx[k];
+        up.Fy[k] = (const R *)sc.Fy[k];
     }
     up.Bxf = (double *)s->Bxf;
     up.Byf = (double *)s->Byf;
     up.Bx0 = sc.Bx0;
     up.By0 = sc.By0;
-    up.Ez = sc.Ez;
+    up.Ez = (const R *)sc.Ez;
     up.dt_dev = dt_dev;
     up.dt_host = dt_host;
     up.a = w[0];
@@ -992,13 +1269,58 @@ void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Sc
     }
 }
 
+template <int LIM>
+static void launch_tubes_lim(int solver, const TubesParams &tp, int blocks, int threads,
+                             cudaStream_t st) {
+    if (solver == HLLD_SOLVER_HLLD)
+        tubes_kernel<LIM, HLLD_SOLVER_HLLD><<<blocks, threads, 0, st>>>(tp);
+    else
+        tubes_kernel<LIM, HLLD_SOLVER_HLLE><<<blocks, threads, 0, st>>>(tp);
+}
+
+void launch_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
+                      void *const *U0, void *const *F, double *t_out, int32_t *steps_out,
+                      unsigned int *next, int threads, int blocks, cudaStream_t st) {
+    TubesParams tp = {};
+    tp.ntubes = b->ntubes;
+    tp.ng = b->ng;
+    tp.max_steps = b->max_steps;
+    tp.scheme = b->scheme;
+    tp.ncells = b->ncells;
+    tp.cell_off = b->cell_off;
+    tp.dx = b->dx;
+    tp.order = b->order;
+    tp.cfl = b->cfl;
+    tp.tend = b->tend;
+    tp.gamma = b->gamma;
+    tp.atmo_rho = b->atmo_rho;
+    for (int k = 0; k < 8; ++k) {
+        tp.U[k] = (double *)cons[k];
+        tp.U0[k] = (double *)U0[k];
+        tp.F[k] = (R *)F[k];
+    }
+    for (int k = 0; k < 9; ++k) tp.P[k] = (R *)prims[k];
+    tp.t_out = t_out;
+    tp.steps_out = steps_out;
+    tp.next = next;
+    cudaMemsetAsync(next, 0, sizeof(unsigned int), st);
+    switch (b->limiter) {
+    case HLLD_LIM_PCM: launch_tubes_lim<HLLD_LIM_PCM>(b->solver, tp, blocks, threads, st); break;
+    case HLLD_LIM_MC: launch_tubes_lim<HLLD_LIM_MC>(b->solver, tp, blocks, threads, st); break;
+    case HLLD_LIM_MINMOD: launch_tubes_lim<HLLD_LIM_MINMOD>(b->solver, tp, blocks, threads, st); break;
+    case HLLD_LIM_WENO5Z: launch_tubes_lim<HLLD_LIM_WENO5Z>(b->solver, tp, blocks, threads, st); break;
+    case HLLD_LIM_MP5: launch_tubes_lim<HLLD_LIM_MP5>(b->solver, tp, blocks, threads, st); break;
+    default: launch_tubes_lim<HLLD_LIM_MP7>(b->solver, tp, blocks, threads, st); break;
+    }
+}
+
 void launch_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,
                           double *dt_dev, unsigned long long *work, cudaStream_t st) {
     Grid G = make_grid(g);
     cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), st);
     SpeedParams sp = {};
     sp.g = G;
-    for (int k = 0; k < 9; ++k) sp.P[k] = (const double *)s->prims[k];
+    for (int k = 0; k < 9; ++k) sp.P[k] = (const R *)s->prims[k];
     sp.out = work;
     speed_kernel<<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(sp);
     dt_kernel<<<1, 1, 0, st>>>(work, g->dx, g->dy, cfl, dt_dev);

@@ -13,6 +13,12 @@
 // C2P and the HLLD p* iteration take their own real type.
 #pragma once
 
+// HLLD_EXACT_ARITH = 1 keeps every division of the reference (the exact,
+// -fmad=false translation unit defines it)
+#ifndef HLLD_EXACT_ARITH
+#define HLLD_EXACT_ARITH 0
+#endif
+
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -78,6 +84,34 @@ template <typename T> __device__ __forceinline__ T sdiv(T num, T den) {
     }
     return num / den;
 }
+
+// Division by a denominator shared by several quotients.  The exact form
+// (HLLD_EXACT_ARITH) divides each numerator as the reference does; the fast
+// forms multiply by one reciprocal of the same safe denominator (the _sdiv
+// tiny-denominator rule is kept), which differs from the quotient by at
+// most one rounding.
+template <typename T> struct SharedDen {
+    T den;  // the safe denominator (exact form) or its reciprocal (fast forms)
+    __device__ __forceinline__ explicit SharedDen(T d) {
+        if (fabs(d) < K<T>::tiny) {
+            T s = tsign(d);
+            if (s == T(0)) s = T(1);
+            d = s * K<T>::tiny;
+        }
+#if HLLD_EXACT_ARITH
+        den = d;
+#else
+        den = T(1) / d;
+#endif
+    }
+    __device__ __forceinline__ T operator()(T num) const {
+#if HLLD_EXACT_ARITH
+        return num / den;
+#else
+        return num * den;
+#endif
+    }
+};
 
 // ── EOS: hybrid_eos(K=0, gamma, gamma_th=gamma) (eos.py:32-76) ───────────
 
@@ -608,23 +642,25 @@ __device__ __forceinline__ void hlld_vars(const HlldR<T> &c, T p, HlldV<T> &o) {
     T XL = BnL * (AL * ncm * BnL + CL) - (AL + GL) * (ncm * p + RTL);
     T XR = BnR * (AR * cx * BnR + CR) - (AR + GR) * (cx * p + RTR);
 
-    T vaL = sdiv(BnL * (AL * BnL + ncm * CL) - (AL + GL) * (p + RSiL), XL);
-    T vaR = sdiv(BnR * (AR * BnR + cx * CR) - (AR + GR) * (p + RSiR), XR);
-    T vt1aL = sdiv(QL * RS1L + RB1L * (CL + BnL * (ncm * RSiL - RTL)), XL);
-    T vt1aR = sdiv(QR * RS1R + RB1R * (CR + BnR * (cx * RSiR - RTR)), XR);
-    T vt2aL = sdiv(QL * RS2L + RB2L * (CL + BnL * (ncm * RSiL - RTL)), XL);
-    T vt2aR = sdiv(QR * RS2R + RB2R * (CR + BnR * (cx * RSiR - RTR)), XR);
+    const SharedDen<T> dXL(XL), dXR(XR);
+    T vaL = dXL(BnL * (AL * BnL + ncm * CL) - (AL + GL) * (p + RSiL));
+    T vaR = dXR(BnR * (AR * BnR + cx * CR) - (AR + GR) * (p + RSiR));
+    T vt1aL = dXL(QL * RS1L + RB1L * (CL + BnL * (ncm * RSiL - RTL)));
+    T vt1aR = dXR(QR * RS1R + RB1R * (CR + BnR * (cx * RSiR - RTR)));
+    T vt2aL = dXL(QL * RS2L + RB2L * (CL + BnL * (ncm * RSiL - RTL)));
+    T vt2aR = dXR(QR * RS2R + RB2R * (CR + BnR * (cx * RSiR - RTR)));
 
-    T Bt1aL = sdiv(RB1L - BnL * vt1aL, ncm - vaL);
-    T Bt1aR = sdiv(RB1R - BnR * vt1aR, cx - vaR);
-    T Bt2aL = sdiv(RB2L - BnL * vt2aL, ncm - vaL);
-    T Bt2aR = sdiv(RB2R - BnR * vt2aR, cx - vaR);
+    const SharedDen<T> dAL(ncm - vaL), dAR(cx - vaR);
+    T Bt1aL = dAL(RB1L - BnL * vt1aL);
+    T Bt1aR = dAR(RB1R - BnR * vt1aR);
+    T Bt2aL = dAL(RB2L - BnL * vt2aL);
+    T Bt2aR = dAR(RB2R - BnR * vt2aR);
 
     T vRS_AL = vaL * RSiL + vt1aL * RS1L + vt2aL * RS2L;
     T vRS_AR = vaR * RSiR + vt1aR * RS1R + vt2aR * RS2R;
 
-    T waL = p + sdiv(RTL - vRS_AL, ncm - vaL);
-    T waR = p + sdiv(RTR - vRS_AR, cx - vaR);
+    T waL = p + dAL(RTL - vRS_AL);
+    T waR = p + dAR(RTR - vRS_AR);
 
     T sqL = sqrt(clamp_lo(waL, T(0)));
     T sqR = sqrt(clamp_lo(waR, T(0)));
@@ -633,20 +669,20 @@ __device__ __forceinline__ void hlld_vars(const HlldR<T> &c, T p, HlldV<T> &o) {
     T dL = ncm * p + RTL - BnL * S_L * sqL;
     T dR = cx * p + RTR + BnR * S_R * sqR;
 
-    T KaL = sdiv(RSiL + p - c.RBiL * S_L * sqL, dL);
-    T KaR = sdiv(RSiR + p + c.RBiR * S_R * sqR, dR);
-    T Kt1aL = sdiv(RS1L - RB1L * S_L * sqL, dL);
-    T Kt1aR = sdiv(RS1R + RB1R * S_R * sqR, dR);
-    T Kt2aL = sdiv(RS2L - RB2L * S_L * sqL, dL);
-    T Kt2aR = sdiv(RS2R + RB2R * S_R * sqR, dR);
+    const SharedDen<T> ddL(dL), ddR(dR);
+    T KaL = ddL(RSiL + p - c.RBiL * S_L * sqL);
+    T KaR = ddR(RSiR + p + c.RBiR * S_R * sqR);
+    T Kt1aL = ddL(RS1L - RB1L * S_L * sqL);
+    T Kt1aR = ddR(RS1R + RB1R * S_R * sqR);
+    T Kt2aL = ddL(RS2L - RB2L * S_L * sqL);
+    T Kt2aR = ddR(RS2R + RB2R * S_R * sqR);
 
     T laL = KaL, laR = KaR;
     T denom_ll = laR - laL;
     T Bic = BnR;
-    T Bt1c = sdiv((Bt1aR * (laR - vaR) + BnR * vt1aR) - (Bt1aL * (laL - vaL) + BnL * vt1aL),
-                  denom_ll);
-    T Bt2c = sdiv((Bt2aR * (laR - vaR) + BnR * vt2aR) - (Bt2aL * (laL - vaL) + BnL * vt2aL),
-                  denom_ll);
+    const SharedDen<T> dll(denom_ll);
+    T Bt1c = dll((Bt1aR * (laR - vaR) + BnR * vt1aR) - (Bt1aL * (laL - vaL) + BnL * vt1aL));
+    T Bt2c = dll((Bt2aR * (laR - vaR) + BnR * vt2aR) - (Bt2aL * (laL - vaL) + BnL * vt2aL));
 
     o.sqL = sqL;
     o.sqR = sqR;
@@ -657,12 +693,12 @@ __device__ __forceinline__ void hlld_vars(const HlldR<T> &c, T p, HlldV<T> &o) {
     o.KaLBc = KaL * Bic + Kt1aL * Bt1c + Kt2aL * Bt2c;
     o.KaRBc = KaR * Bic + Kt1aR * Bt1c + Kt2aR * Bt2c;
     if (FULL) {
-        T DaL = sdiv(c.RDL, ncm - vaL);
-        T DaR = sdiv(c.RDR, cx - vaR);
+        T DaL = dAL(c.RDL);
+        T DaR = dAR(c.RDR);
         T vBaL = vaL * BnL + vt1aL * Bt1aL + vt2aL * Bt2aL;
         T vBaR = vaR * BnR + vt1aR * Bt1aR + vt2aR * Bt2aR;
-        T TauaL = sdiv(RTL + p * vaL - vBaL * BnL, ncm - vaL) - DaL;
-        T TauaR = sdiv(RTR + p * vaR - vBaR * BnR, cx - vaR) - DaR;
+        T TauaL = dAL(RTL + p * vaL - vBaL * BnL) - DaL;
+        T TauaR = dAR(RTR + p * vaR - vBaR * BnR) - DaR;
         o.SaL = (TauaL + DaL + p) * vaL - vBaL * BnL;
         o.SaR = (TauaR + DaR + p) * vaR - vBaR * BnR;
         o.St1aL = (TauaL + DaL + p) * vt1aL - vBaL * Bt1aL;

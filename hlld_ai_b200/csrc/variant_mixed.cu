@@ -1,0 +1,10 @@
+// Mixed-precision variant: FP32 primitives, reconstruction, physical
+// fluxes, HLL state, HLL-state C2P (the p* bracket seed), star states, corner
+// EMF and flux divergence; FP64 HLLD p* iteration, cell C2P and RK
+// accumulation of the conserved state and the staggered field.
+#define HLLD_NS v_mixed
+#define HLLD_REAL float
+#ifndef HLLD_BRACKET_REAL
+#define HLLD_BRACKET_REAL float
+#endif
+#include "kernels_impl.cuh"

@@ -1,6 +1,8 @@
 // Launchers exported by each arithmetic variant of kernels_impl.cuh.
 // v_fp64: FP64 with FMA contraction; v_exact: FP64 with one rounding per
-// operation (translation unit built with -fmad=false).
+// operation (translation unit built with -fmad=false); v_mixed: FP32
+// primitives, reconstruction, fluxes, EMF and divergence, FP64 cell C2P,
+// HLLD p* iteration and RK accumulation.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -11,9 +13,9 @@ namespace hlld {
 
 // Scratch arrays of one 2D step (carved out of the caller's buffer).
 struct Scratch2D {
-    double *Fx[7];  // x-face fluxes: D, Sx, Sy, Sz, tau, Bz, By
-    double *Fy[7];  // y-face fluxes: D, Sx, Sy, Sz, tau, Bz, Bx
-    double *Ez;     // corner EMF
+    void *Fx[7];  // x-face fluxes: D, Sx, Sy, Sz, tau, Bz, By (the variant's real type)
+    void *Fy[7];  // y-face fluxes: D, Sx, Sy, Sz, tau, Bz, Bx
+    void *Ez;     // corner EMF (the variant's real type)
     double *U0[6];  // RK stage-0 copy of the evolved cell variables
     double *Bx0, *By0;
     hlld_step_diag_t *diag;  // used when the caller passes none
@@ -38,7 +40,10 @@ struct Scratch2D {
     void launch_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,        \
                               double *dt_dev, unsigned long long *work, cudaStream_t st);         \
     void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis,                \
-                        double *const *F, hlld_flux_diag_t *fdiag, cudaStream_t st);              \
+                        void *const *F, hlld_flux_diag_t *fdiag, cudaStream_t st);                \
+    void launch_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,           \
+                          void *const *U0, void *const *F, double *t_out, int32_t *steps_out,     \
+                          unsigned int *next, int threads, int blocks, cudaStream_t st);          \
     void launch_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,  \
                             const hlld_step_diag_t *diag, int stage, int scheme, double dt_host,  \
                             const double *dt_dev, cudaStream_t st);                               \
@@ -49,5 +54,6 @@ int report_error(int code, const char *fmt, ...);
 
 HLLD_DECLARE_VARIANT(v_fp64)
 HLLD_DECLARE_VARIANT(v_exact)
+HLLD_DECLARE_VARIANT(v_mixed)
 
 }  // namespace hlld

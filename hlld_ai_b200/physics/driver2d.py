@@ -40,8 +40,12 @@ class Stepper2D:
             raise ValueError(f"unknown boundary condition {(bc_x, bc_y)!r}")
         if limiter not in _lib.LIMITERS:
             raise ValueError(f"unknown limiter {limiter!r}")
-        if precision not in ("fp64", "fp64_exact"):
-            raise NotImplementedError(f"precision {precision!r} for the 2D step")
+        if precision not in ("fp64", "fp64_exact", "mixed"):
+            raise ValueError(f"unknown precision {precision!r}")
+        self.precision = precision
+        # mixed: primitives (and the step's fluxes) are float32; the conserved
+        # state and the staggered field stay float64
+        self.prim_dtype = torch.float32 if precision == "mixed" else torch.float64
         self.grid = grid
         self.device = torch.device(grid.device)
         if self.device.type != "cuda":
@@ -71,16 +75,16 @@ class Stepper2D:
         for i, k in enumerate(EVOLVED_KEYS):
             s.cons[i] = self._check(state.cons[k], cs, f"cons[{k!r}]")
         for i, k in enumerate(PRIM_KEYS):
-            s.prims[i] = self._check(state.prims[k], cs, f"prims[{k!r}]")
+            s.prims[i] = self._check(state.prims[k], cs, f"prims[{k!r}]", self.prim_dtype)
         s.Bxf = self._check(state.Bxf, fx, "Bxf")
         s.Byf = self._check(state.Byf, fy, "Byf")
         return s
 
-    def _check(self, t, shape, name) -> int:
+    def _check(self, t, shape, name, dtype=torch.float64) -> int:
         if not isinstance(t, torch.Tensor) or not t.is_cuda or t.device != self.device:
             raise TypeError(f"{name} must be a CUDA tensor on {self.device}")
-        if t.dtype != torch.float64 or tuple(t.shape) != shape or not t.is_contiguous():
-            raise ValueError(f"{name} must be contiguous float64 {shape}, got "
+        if t.dtype != dtype or tuple(t.shape) != shape or not t.is_contiguous():
+            raise ValueError(f"{name} must be contiguous {dtype} {shape}, got "
                              f"{t.dtype} {tuple(t.shape)}")
         return t.data_ptr()
 
@@ -90,7 +94,9 @@ class Stepper2D:
         for k in PRIM_KEYS:
             t = state.prims.get(k)
             if t is None or not t.is_contiguous() or tuple(t.shape) != (g.nxt, g.nyt):
-                state.prims[k] = torch.zeros(g.nxt, g.nyt, dtype=torch.float64, device=self.device)
+                state.prims[k] = torch.zeros(g.nxt, g.nyt, dtype=self.prim_dtype, device=self.device)
+            elif t.dtype != self.prim_dtype:
+                state.prims[k] = t.to(self.prim_dtype).contiguous()
 
     # -- operations ---------------------------------------------------------
     def step(self, state: State2D, dt, scheme: str = "rk3") -> None:

@@ -173,7 +173,10 @@ def setup_problem(problem: str, n: int, *, limiter: str = "mc", device="cuda",
     g = Grid2D(gc.xmin, gc.xmax, n, gc.ymin, gc.ymax, n, ng=ng, device=device)
     prims = {k: v.contiguous().to(device) for k, v in prims.items()}
     Bxf, Byf = b_from_potential(Az.to(device), g.dx, g.dy)
-    c = prims_to_cons_2d(prims, g, precision)
+    # conserved variables from the FP64 initial primitives in every precision
+    c = prims_to_cons_2d(prims, g, "fp64_exact" if precision == "fp64_exact" else "fp64")
+    if precision == "mixed":
+        prims = {k: v.to(torch.float32).contiguous() for k, v in prims.items()}
     st = State2D(cons={k: c[k].contiguous() for k in EVOLVED_KEYS}, Bxf=Bxf.contiguous(),
                  Byf=Byf.contiguous(), prims=prims)
     st = sync_state(st, g, eos, *spec["bc"], precision=precision, limiter=limiter)

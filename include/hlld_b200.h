@@ -107,6 +107,24 @@ typedef struct {
     void *prims[9];
 } hlld_state2d_t;
 
+/* A batch of independent 1D tubes (the batched-tube workload): tube i has
+ * ncells[i] physical cells and ng ghosts per side, occupies cells
+ * cell_off[i] .. cell_off[i] + ncells[i] + 2 ng - 1 of the concatenated cell
+ * arrays and faces cell_off[i] + i .. cell_off[i] + i + ncells[i] + 2 ng of
+ * the face arrays, and has cell width dx[i].  order (may be NULL) is the
+ * processing order (e.g. longest tube first).  All pointers are device. */
+typedef struct {
+    int32_t ntubes, ng;
+    const int32_t *ncells;
+    const int64_t *cell_off;
+    const double *dx;
+    const int32_t *order;
+    double cfl, tend;
+    int32_t max_steps;
+    int32_t limiter, solver, scheme, precision;
+    double gamma, atmo_rho;
+} hlld_tubes_t;
+
 int hlld_version(void);
 const char *hlld_error_string(int code);
 const char *hlld_last_error_detail(void);
@@ -190,6 +208,21 @@ int hlld_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *cons
                      void *const *Fy, void *Ez, void *const *U0, void *Bx0, void *By0,
                      const hlld_step_diag_t *diag, int stage, int scheme, double dt_host,
                      const double *dt_dev, void *stream);
+
+/* Replaces src/physics/tube_seed.py:93-144 run_tubes for the batched-tube
+ * workload, with a dt per tube: every tube runs src/physics/driver2d.py:309-355
+ * rk_step on a ny = 1 grid (x sweep only -- the y sweep of a ny = 1 grid
+ * contributes exactly zero), dt from src/physics/driver.py:77-127
+ * compute_dt each step, until tend or max_steps, in ONE persistent launch of
+ * `blocks` CTAs of `threads` threads (0 = library defaults).  prims (9
+ * arrays, ghosts filled) are read and updated in place; cons (8), U0 (8
+ * cell arrays) and F (8 face arrays, slot Bx unused) are work arrays;
+ * t_out / steps_out get each tube's final time and step count; next is one
+ * device unsigned int (the work counter, zeroed by the call).  Primitives
+ * and F are float for HLLD_MIXED, double otherwise. */
+int hlld_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
+                   void *const *U0, void *const *F, double *t_out, int32_t *steps_out,
+                   unsigned int *next, int threads, int blocks, void *stream);
 
 /* Replaces src/physics/driver2d.py:251-281 compute_dt_2d: writes
  * dt = cfl / (max(|vx|+cf)/dx + max(|vy|+cf)/dy) to dt_dev (device double);

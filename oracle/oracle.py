@@ -228,3 +228,19 @@ def rk2_step_1d(cons: dict, prims: dict, ncells: int, ng: int, dx: float, dt: fl
                           ctypes.c_double(dt), ctypes.c_int(LIMITERS[limiter]),
                           ctypes.c_int(SOLVERS[solver]), ctypes.c_double(gamma),
                           ctypes.c_double(atmo_rho), C, P)
+
+
+def tube_run(prims: dict, L: int, ng: int, dx: float, cfl: float, tend: float, limiter: str,
+             solver: str, gamma: float, scheme: str = "rk3", max_steps: int = 1 << 30,
+             atmo_rho: float = 1e-10):
+    """One 1D tube to tend (driver2d.py:309-355 on a ny = 1 grid), in place
+    on 9 primitive arrays of L + 2 ng cells; returns (t, steps)."""
+    P = _ptrs([prims[k] for k in PRIM_KEYS])
+    t = ctypes.c_double(0.0)
+    steps = lib().orc_tube_run(ctypes.c_int(L), ctypes.c_int(ng), ctypes.c_double(dx),
+                               ctypes.c_double(cfl), ctypes.c_double(tend),
+                               ctypes.c_int(max_steps), ctypes.c_int(LIMITERS[limiter]),
+                               ctypes.c_int(SOLVERS[solver]), ctypes.c_double(gamma),
+                               ctypes.c_double(atmo_rho), ctypes.c_int(3 if scheme == "rk3" else 2),
+                               P, ctypes.byref(t))
+    return t.value, int(steps)

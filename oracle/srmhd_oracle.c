@@ -1495,3 +1495,95 @@ void orc_rk2_step_1d(int ncells, int ng, double dx, double dt, int limiter, int 
     }
     for (int k = 0; k < ORC_NPRIM; ++k) free(p1[k]);
 }
+
+/* ── batched-tube workload: one 1D tube (driver2d.py:309-355 on ny = 1) ─ */
+
+/* driver.py:77-127 compute_dt with speed_of_light = False; `(cfl*dx) /
+ * tensor` is torch's reciprocal(tensor) * (cfl*dx) */
+static double tube_dt(int L, int ng, double dx, double cfl, double gamma,
+                      const double *const *prim) {
+    double mx = 0.0;
+    int first = 1, nan_seen = 0;
+    for (int i = ng; i < ng + L; ++i) {
+        double rho = prim[ORC_RHO][i], eps = prim[ORC_EPS][i];
+        double vx = prim[ORC_VX][i], vy = prim[ORC_VY][i], vz = prim[ORC_VZ][i];
+        double Bx = prim[ORC_PBX][i], By = prim[ORC_PBY][i], Bz = prim[ORC_PBZ][i];
+        double p, cs2;
+        eos_press_cs2(eps, rho, gamma, &p, &cs2);
+        double v2 = vx * vx + vy * vy + vz * vz;
+        double W = 1.0 / sqrt(clamp_lo(1.0 - v2, 1e-10));
+        double B2 = Bx * Bx + By * By + Bz * Bz;
+        double vdotB = vx * Bx + vy * By + vz * Bz;
+        double b2 = (B2 + vdotB * vdotB) / (W * W);
+        double h = 1.0 + eps + p / rho;
+        double v02 = cs2 + (b2 / (rho * h + b2)) * (1.0 - cs2);
+        double vf = sqrt(clamp_hi(clamp_lo(v02, 0.0), 1.0));
+        double s = fabs(vx) + vf;
+        if (isnan(s)) nan_seen = 1;
+        if (first || s > mx) mx = s;
+        first = 0;
+    }
+    if (nan_seen) return NAN;
+    mx = clamp_lo(mx, 1e-14);
+    return (1.0 / mx) * (cfl * dx);
+}
+
+int orc_tube_run(int L, int ng, double dx, double cfl, double tend, int max_steps, int limiter,
+                 int solver, double gamma, double atmo_rho, int scheme, double *const *prim,
+                 double *t_out) {
+    const int nt = L + 2 * ng, nf = nt + 1;
+    const double(*tab)[3] = scheme == 3 ? RK3 : RK2;
+    const int nst = scheme == 3 ? 3 : 2;
+    double *U[ORC_NCONS], *U0[ORC_NCONS], *F[ORC_NCONS], *Uf[ORC_NCONS];
+    double *Lp[ORC_NPRIM], *Rp[ORC_NPRIM];
+    for (int k = 0; k < ORC_NCONS; ++k) {
+        U[k] = (double *)malloc(sizeof(double) * nt);
+        U0[k] = (double *)malloc(sizeof(double) * nt);
+        F[k] = (double *)malloc(sizeof(double) * nf);
+        Uf[k] = (double *)malloc(sizeof(double) * nf);
+    }
+    for (int k = 0; k < ORC_NPRIM; ++k) {
+        Lp[k] = (double *)malloc(sizeof(double) * nf);
+        Rp[k] = (double *)malloc(sizeof(double) * nf);
+    }
+    double *ps = (double *)malloc(sizeof(double) * nf);
+    orc_prim_to_cons(nt, (const double *const *)prim, U);
+    double t = 0.0;
+    int steps = 0;
+    while (t < tend - 1e-14 && steps < max_steps) {
+        double dt = tube_dt(L, ng, dx, cfl, gamma, (const double *const *)prim);
+        if (dt > tend - t) dt = tend - t;
+        if (!(dt > 0.0)) break;
+        for (int k = 0; k < ORC_NCONS; ++k) memcpy(U0[k], U[k], sizeof(double) * nt);
+        for (int st = 0; st < nst; ++st) {
+            double a = tab[st][0], b = tab[st][1], c = tab[st][2];
+            /* sweep.py:30-119 with Bnf = None: all eight work variables */
+            orc_reconstruct_prims((const double *const *)prim, nt, 1, 0, limiter, 1, gamma, Lp, Rp);
+            orc_riemann(nf, (const double *const *)Lp, (const double *const *)Rp, 0, solver, gamma,
+                        F, Uf, ps, NULL, NULL, NULL);
+            for (int e = 0; e < nf; ++e) F[ORC_BX][e] = 0.0;
+            double w2 = c * dt;
+            for (int k = 0; k < ORC_NCONS; ++k)
+                for (int i = 0; i < nt; ++i) {
+                    /* rx + ry with ry = -0.0 exactly (identical y faces) */
+                    double rhs = -(F[k][i + 1] - F[k][i]) / dx + (-0.0);
+                    double v = a * U0[k][i] + b * U[k][i];
+                    U[k][i] = v + w2 * rhs;
+                }
+            for (int k = 0; k < ORC_NCONS; ++k) outflow_1d(U[k], L, ng);
+            orc_cons_to_prim(nt, (const double *const *)U, gamma, atmo_rho, 1e-10, prim, NULL);
+            for (int k = 0; k < ORC_NPRIM; ++k) outflow_1d(prim[k], L, ng);
+        }
+        t += dt;
+        steps++;
+    }
+    if (t_out) *t_out = t;
+    for (int k = 0; k < ORC_NCONS; ++k) {
+        free(U[k]); free(U0[k]); free(F[k]); free(Uf[k]);
+    }
+    for (int k = 0; k < ORC_NPRIM; ++k) {
+        free(Lp[k]); free(Rp[k]);
+    }
+    free(ps);
+    return steps;
+}

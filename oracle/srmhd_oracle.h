@@ -133,6 +133,18 @@ void orc_corner_emf(int n0, int n1, const double *Ec, const double *Efx, const d
 void orc_rk2_step_1d(int ncells, int ng, double dx, double dt, int limiter, int solver,
                      double gamma, double atmo_rho, double *const *cons, double *const *prim);
 
+/* One 1D tube run to tend (the batched-tube workload): driver2d.py:309-355
+ * rk_step (no CT) on a ny = 1 grid, whose y sweep contributes exactly zero,
+ * so only the x sweep is formed: reconstruct_prims of all eight work
+ * variables (W v), flux_fn with idir 0, F[Bx] = 0, all eight conserved
+ * variables evolved, outflow BCs, C2P, P[B] = U[B].  dt per step is
+ * driver.py:77-127 compute_dt (max |vx| + c_f over the physical cells),
+ * capped at tend - t.  prim: 9 arrays of L + 2 ng cells (ghosts filled),
+ * updated in place.  Returns the number of steps taken. */
+int orc_tube_run(int L, int ng, double dx, double cfl, double tend, int max_steps, int limiter,
+                 int solver, double gamma, double atmo_rho, int scheme, double *const *prim,
+                 double *t_out);
+
 #ifdef __cplusplus
 }
 #endif

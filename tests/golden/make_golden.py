@@ -16,6 +16,8 @@ inputs, the outputs the oracle is pinned against (tests/test_oracle_golden.py):
   ct.npz       corner_emf() on random EMFs and mass fluxes (upwind on/off)
   step2d.npz   sync_state + two rk_step_ct steps of four small 2D problems
   tube1d.npz   six rk2_step steps of the 800-cell Brio-Wu tube (PLM-MC, HLLD)
+  tubes.npz    three batched-workload tubes (WENO5-Z, HLLD, SSP-RK3): driver2d
+               rk_step on ny = 1 grids with driver.compute_dt, four steps each
 
 The reference is not needed to run the tests; only this script reads it.
 """
@@ -248,6 +250,44 @@ def main(ref_root: str) -> None:
     out.update({f"cons_{k}": cons[k].numpy() for k in cons})
     out["dt"] = np.float64(dt)
     np.savez_compressed(os.path.join(HERE, "tube1d.npz"), **out)
+
+    # ── batched-workload tubes (driver2d.rk_step on ny = 1, driver.compute_dt) ──
+    from src.physics.driver import compute_dt
+    from src.physics.driver2d import rk_step
+    out = {}
+    gen = np.random.default_rng(20261203)
+    for ti, L in enumerate((64, 96, 128)):
+        e = hybrid_eos(K=0.0, gamma=G, gamma_th=G)
+        gr = Grid2D(0.0, 1.0, L, 0.0, 1.0, 1, ng=3)
+        rho = 10.0 ** gen.uniform(-1, 1, 2)
+        p = 10.0 ** gen.uniform(-2, 2, 2)
+        v = gen.uniform(-0.5, 0.5, (2, 3))
+        Bt = gen.uniform(-2, 2, (2, 2))
+        bx = gen.uniform(-1, 1)
+        left = gr.X < 0.5
+        pick = lambda a, b: torch.where(left, torch.full_like(gr.X, float(a)), torch.full_like(gr.X, float(b)))
+        prims = {"rho": pick(rho[0], rho[1]), "p": pick(p[0], p[1]),
+                 "vx": pick(v[0, 0], v[1, 0]), "vy": pick(v[0, 1], v[1, 1]),
+                 "vz": pick(v[0, 2], v[1, 2]), "Bx": torch.full_like(gr.X, float(bx)),
+                 "By": pick(Bt[0, 0], Bt[1, 0]), "Bz": pick(Bt[0, 1], Bt[1, 1])}
+        prims = {k: vv.contiguous().clone() for k, vv in prims.items()}
+        prims["eps"] = e.eps__press_rho(prims["p"], prims["rho"])
+        for k in PK:
+            out[f"t{ti}_init_{k}"] = prims[k][:, 3].numpy().copy()
+        cons = prims_to_cons_2d(prims, gr)
+        cons = {k: cons[k] for k in CK}
+        dts = []
+        for _ in range(4):
+            row = {k: prims[k][:, 3] for k in PK}
+            dt = float(compute_dt(row, e, gr.dx, 0.4, gr.ng, L))
+            dts.append(dt)
+            cons, prims, _ = rk_step(cons, prims, gr, e, dt, scheme="rk3", bc_x="outflow",
+                                     bc_y="periodic", limiter="weno5z")
+        out[f"t{ti}_dt"] = np.array(dts)
+        out[f"t{ti}_L"] = np.int64(L)
+        for k in PK:
+            out[f"t{ti}_prims_{k}"] = prims[k][:, 3].numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "tubes.npz"), **out)
     print("golden vectors written to", HERE)
 
 

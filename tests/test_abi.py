@@ -43,8 +43,8 @@ PROBE = r"""
 #include <stddef.h>
 #include "hlld_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu\n", sizeof(hlld_flux_diag_t), sizeof(hlld_step_diag_t),
-         sizeof(hlld_grid2d_t), sizeof(hlld_state2d_t));
+  printf("%zu %zu %zu %zu %zu\n", sizeof(hlld_flux_diag_t), sizeof(hlld_step_diag_t),
+         sizeof(hlld_grid2d_t), sizeof(hlld_state2d_t), sizeof(hlld_tubes_t));
   printf("%zu %zu %zu %zu %zu\n", offsetof(hlld_grid2d_t, dx), offsetof(hlld_grid2d_t, gamma),
          offsetof(hlld_grid2d_t, upwind), offsetof(hlld_state2d_t, Bxf),
          offsetof(hlld_step_diag_t, speed_max_bits));
@@ -62,10 +62,11 @@ def test_struct_layouts_match_ctypes(tmp_path):
     subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)],
                    check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
-    sizes = [int(x) for x in out[:4]]
-    offs = [int(x) for x in out[4:]]
+    sizes = [int(x) for x in out[:5]]
+    offs = [int(x) for x in out[5:]]
     assert sizes == [ctypes.sizeof(_lib.FluxDiag), ctypes.sizeof(_lib.StepDiag),
-                     ctypes.sizeof(_lib.Grid2DC), ctypes.sizeof(_lib.State2DC)]
+                     ctypes.sizeof(_lib.Grid2DC), ctypes.sizeof(_lib.State2DC),
+                     ctypes.sizeof(_lib.TubesC)]
     assert offs == [_lib.Grid2DC.dx.offset, _lib.Grid2DC.gamma.offset, _lib.Grid2DC.upwind.offset,
                     _lib.State2DC.Bxf.offset, _lib.StepDiag.speed_max_bits.offset]
 
@@ -90,7 +91,7 @@ def test_scratch_size_and_argument_errors_without_gpu():
         rc = L.hlld_step2d_scratch_bytes(ctypes.byref(gb), ctypes.byref(n))
         assert rc == _lib.HLLD_OK - 1, bad  # HLLD_ERR_INVALID
         assert L.hlld_last_error_detail()
-    gm = grid(precision=2)
+    gm = grid(precision=9)
     assert L.hlld_step2d_scratch_bytes(ctypes.byref(gm), ctypes.byref(n)) == -3
     s = _lib.State2DC()
     # NULL state arrays and NULL scratch are rejected on the host
@@ -100,6 +101,18 @@ def test_scratch_size_and_argument_errors_without_gpu():
                                 None, None, None) == -1
     assert L.hlld_cons_to_prim(10, None, 5 / 3, 1e-10, 1e-10, 0, None, None, None) == -1
     assert L.hlld_error_string(-4) == b"scratch buffer too small"
+
+
+def test_tube_batch_argument_errors_without_gpu():
+    L = _lib.lib()
+    empty = _lib.TubesC(ntubes=0, ng=3, cfl=0.4, tend=0.1, limiter=3, solver=1, scheme=3,
+                        gamma=5 / 3)
+    assert L.hlld_tubes_run(ctypes.byref(empty), None, None, None, None, None, None, None, 0, 0,
+                            None) == 0
+    b = _lib.TubesC(ntubes=4, ng=3, cfl=0.4, tend=0.1, limiter=3, solver=1, scheme=3, gamma=5 / 3)
+    assert L.hlld_tubes_run(ctypes.byref(b), None, None, None, None, None, None, None, 0, 0,
+                            None) == -1
+    assert L.hlld_tubes_run(None, None, None, None, None, None, None, None, 0, 0, None) == -1
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):

@@ -193,3 +193,18 @@ def test_brio_wu_rk2_matches_reference():
         assert max_rel(z[f"prims_{k}"], prims[k]) < 1e-11, k
     for k in CK:
         assert max_rel(z[f"cons_{k}"], cons[k]) < 1e-11, k
+
+
+@pytest.mark.parametrize("ti", [0, 1, 2])
+def test_tube_runs_match_reference(ti):
+    """The batched-workload tube (driver2d.rk_step on a ny = 1 grid, WENO5-Z,
+    HLLD, SSP-RK3, driver.compute_dt per step): four steps."""
+    z = load("tubes.npz")
+    L = int(z[f"t{ti}_L"])
+    prims = {k: z[f"t{ti}_init_{k}"].copy() for k in PK}
+    t, steps = oracle.tube_run(prims, L, 3, 1.0 / L, 0.4, 10.0, "weno5z", "hlld", 5.0 / 3.0,
+                               max_steps=4)
+    assert steps == 4
+    assert abs(t - float(np.sum(z[f"t{ti}_dt"]))) <= 1e-12 * t
+    for k in PK:
+        assert max_rel(z[f"t{ti}_prims_{k}"], prims[k]) < 1e-11, k
