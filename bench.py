@@ -56,6 +56,12 @@ def parse():
     ap.add_argument("--cpu-n", type=int, default=512, help="grid of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="rotor", choices=["rotor", "tubes"],
+                    help="rotor: the 2D rotor step (default); tubes: the batched-tube launch")
+    ap.add_argument("--tubes", type=int, default=4096)
+    ap.add_argument("--chunk", type=float, default=0.01,
+                    help="tubes: simulated time every tube advances per step")
+    ap.add_argument("--cpu-tubes", type=int, default=12, help="tubes of the CPU baseline sample")
     return ap.parse_args()
 
 
@@ -419,10 +425,167 @@ def run_ours(a):
     return 0
 
 
+# ── batched tubes ────────────────────────────────────────────────────────────
+
+TUBES_WORKLOAD = ("batched 1D SRMHD tubes, lengths uniform in [256, 4096], seeded left/right "
+                  "states, gamma 5/3, WENO5-Z + HLLD + SSP-RK3, per-tube CFL 0.4 dt")
+
+
+def tubes_cpu_sample(states, ntubes, chunk):
+    """cell-updates/s of the oracle advancing a seeded subset of the tubes by
+    `chunk` (one tube at a time, one thread)."""
+    from oracle import oracle
+    from hlld_ai_b200.tubes import tube_prims
+
+    idx = list(range(0, len(states.lengths), max(1, len(states.lengths) // ntubes)))[:ntubes]
+    work, secs = 0, 0.0
+    for i in idx:
+        p = tube_prims(states, i, 3)
+        L = int(states.lengths[i])
+        t0 = time.perf_counter()
+        _, steps = oracle.tube_run(p, L, 3, 1.0 / L, 0.4, chunk, "weno5z", "hlld", 5.0 / 3.0)
+        secs += time.perf_counter() - t0
+        work += L * steps
+    return work / secs, len(idx), work
+
+
+def run_tubes(a):
+    """One step = one replay of the CUDA graph holding the persistent launch,
+    which advances every tube by `chunk` of simulated time (each tube with its
+    own CFL steps).  value = physical cell-updates (cells x RK3 steps summed
+    over tubes) per second."""
+    import torch
+    import torch.distributed as dist
+
+    from hlld_ai_b200.tubes import TubeBatch, random_tubes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev,
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    # tubes are independent units: each rank runs its own seeded batch
+    states = random_tubes(a.tubes, seed=20261203 + rank)
+    precision = "mixed" if a.precision == "mixed" else a.precision
+    b = TubeBatch(states, limiter="weno5z", solver="hlld", scheme="rk3", precision=precision,
+                  device=dev)
+    tuned = b.autotune(tend=a.chunk / 4, sample=1024)
+    g = b.capture(tend=a.chunk)
+    b.reset()
+    L = torch.as_tensor(states.lengths, dtype=torch.int64, device=dev)
+    acc = torch.zeros(a.tubes, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(a.warmup):
+        g.replay()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(dev.index or 0)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    kernel_ms = []
+    e0.record(stream)
+    for _ in range(a.steps):
+        k0.record(stream)
+        g.replay()
+        k1.record(stream)
+        acc += b.steps_out
+        k1.synchronize()
+        kernel_ms.append(k0.elapsed_time(k1))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    updates = int((acc * L).sum().item())
+    if world > 1:
+        m = torch.tensor([ms, float(updates)], dtype=torch.float64, device=dev)
+        mx = m.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(m, op=dist.ReduceOp.SUM)
+        ms, updates = float(mx[0].item()), int(m[1].item())
+    value = updates / (ms * 1e-3)
+    # algorithmic bytes per cell-update: per stage read P (7 words, storage
+    # precision) and U (7 FP64), write both; stages 2 and 3 also read U0
+    rb = 4 if precision == "mixed" else 8
+    bytes_per_update = 3 * (14 * rb + 14 * 8) // 1 + 2 * 7 * 8
+    kernel_s = 1e-3 * sum(kernel_ms) / len(kernel_ms)
+    achieved = bytes_per_update * (updates / world / a.steps) / kernel_s / 1e9
+    peak, peak_kind = peaks()
+
+    # end to end: host primitives -> device, the launch, primitives -> host
+    host = {k: torch.empty_like(v, device="cpu").pin_memory() for k, v in b.prims.items()}
+    for k, v in b.prims.items():
+        host[k].copy_(v)
+    nbytes = sum(h.numel() * h.element_size() for h in host.values())
+    ke = max(1, min(a.steps, 3))
+    acc.zero_()
+    torch.cuda.synchronize(dev)
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(ke):
+        for k, v in b.prims.items():
+            v.copy_(host[k], non_blocking=True)
+        b.launch(tend=a.chunk)
+        acc += b.steps_out
+        for k, v in b.prims.items():
+            host[k].copy_(v, non_blocking=True)
+    f1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_updates = int((acc * L).sum().item()) * world
+    e2e = {"value": e2e_updates / (f0.elapsed_time(f1) * 1e-3), "unit": "cell-updates/s",
+           "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ke,
+           "path": "TubeBatch.launch with pinned host primitives"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        v, nt, work = tubes_cpu_sample(states, a.cpu_tubes, a.chunk)
+        cpu = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+               "sample": f"{nt} of the tubes advanced by {a.chunk} ({work} cell-updates), "
+                         "C oracle, one thread"}
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if precision == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": TUBES_WORKLOAD, "tubes": a.tubes, "chunk": a.chunk,
+                       "precision": precision, "threads": tuned[0], "blocks": tuned[1],
+                       "total_cells": b.total_cells, "parallelism": f"replicas x{world}",
+                       "l2": "state of the batch above L2 (~0.7 GB), no flush"},
+            "e2e": e2e,
+            "gpu_launches": a.steps,
+            "roofline": {"bound": "hbm", "kernel": "tubes_kernel", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "bytes_per_cell_update": bytes_per_update,
+                         "avg_launch_ms": kernel_s * 1e3},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "tubes":
+        return run_tubes(a)
     return run_ours(a)
 
 

@@ -59,7 +59,11 @@ class TubesC(ctypes.Structure):
                 ("max_steps", ctypes.c_int32), ("limiter", ctypes.c_int32),
                 ("solver", ctypes.c_int32), ("scheme", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("gamma", ctypes.c_double),
-                ("atmo_rho", ctypes.c_double)]
+                ("atmo_rho", ctypes.c_double), ("flavor", ctypes.c_int32),
+                ("resume", ctypes.c_int32)]
+
+
+TUBE_RK_STEP, TUBE_DRIVER1D_LIGHT, TUBE_DRIVER1D_CFL = 0, 1, 2
 
 
 # exported symbol -> (restype, argtypes)

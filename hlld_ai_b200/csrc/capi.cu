@@ -292,6 +292,8 @@ int hlld_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
     if (b->solver != HLLD_SOLVER_HLLE && b->solver != HLLD_SOLVER_HLLD)
         return fail(HLLD_ERR_INVALID, "solver must be HLLE or HLLD");
     if (b->scheme != 2 && b->scheme != 3) return fail(HLLD_ERR_INVALID, "scheme must be 2 or 3");
+    if (b->flavor < HLLD_TUBE_RK_STEP || b->flavor > HLLD_TUBE_DRIVER1D_CFL)
+        return fail(HLLD_ERR_INVALID, "unknown tube flavor %d", b->flavor);
     if (!(b->gamma > 1.0) || !(b->cfl > 0.0)) return fail(HLLD_ERR_INVALID, "gamma, cfl");
     if (!step_precision(b->precision)) return fail(HLLD_ERR_UNSUPPORTED, "precision %d", b->precision);
     for (int k = 0; k < 8; ++k)

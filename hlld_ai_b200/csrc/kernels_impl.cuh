@@ -143,6 +143,18 @@ template <typename T> __device__ __forceinline__ T weno5z(T vm2, T vm1, T v0, T 
     T tau5 = fabs(b0 - b2);
     const T eps = K<T>::weno_eps;
     T r0 = tau5 / (b0 + eps), r1 = tau5 / (b1 + eps), r2 = tau5 / (b2 + eps);
+    if constexpr (sizeof(T) == 4) {
+        // FP32: r^2 overflows once r > 1.8e19 (a smooth stencil next to a
+        // jump has beta = 0); the weights are normalised, so divide every
+        // 1 + r^2 by the largest (1 + r^2) scale first
+        T s = tmax(T(1), tmax(r0, tmax(r1, r2)));
+        T is = T(1) / s, i2 = is * is;
+        T q0 = r0 * is, q1 = r1 * is, q2 = r2 * is;
+        T a0 = T(0.1) * (i2 + q0 * q0);
+        T a1 = T(0.6) * (i2 + q1 * q1);
+        T a2 = T(0.3) * (i2 + q2 * q2);
+        return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
+    }
     T a0 = T(0.1) * (T(1) + r0 * r0);
     T a1 = T(0.6) * (T(1) + r1 * r1);
     T a2 = T(0.3) * (T(1) + r2 * r2);
@@ -775,6 +787,8 @@ __constant__ double kRK2d[2][3] = {{1.0, 0.0, 1.0}, {0.5, 0.5, 0.5}};
 
 struct TubesParams {
     int ntubes, ng, max_steps, scheme;
+    int light;      // driver flavors: max speed taken as 1 (dt = cfl dx)
+    int resume;     // cons already valid: skip the prim -> cons at launch
     const int32_t *ncells;
     const int64_t *cell_off;  // first cell (ghosts included) of each tube
     const double *dx;
@@ -879,6 +893,40 @@ __device__ __forceinline__ void tube_face(const TubesParams &p, int64_t base, in
         if (k != C_BX) p.F[k][fout] = o.F[k];
 }
 
+// One physical face of the 1D shock-tube driver (driver.py:130-189,
+// reconstruction.py:354-373): every primitive, eps included, reconstructed
+// as it is along the whole line (no W v, no positivity fallback, no floors).
+template <int LIM, int SOLVER>
+__device__ __forceinline__ void tube_face_driver1d(const TubesParams &p, int64_t base, int nt, int f,
+                                                   int64_t fout) {
+    using T = R;
+    constexpr int S = Stencil<LIM>::S;
+    constexpr int NW = 2 * S + 2;
+    int cw[NW];
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        int c = f - 1 - S + k;
+        cw[k] = c < 0 ? 0 : (c > nt - 1 ? nt - 1 : c);
+    }
+    T PL[NPRIM], PR[NPRIM];
+#pragma unroll
+    for (int v = 0; v < NPRIM; ++v) {
+        T w[NW];
+#pragma unroll
+        for (int k = 0; k < NW; ++k) w[k] = p.P[v][base + cw[k]];
+        PL[v] = cell_edge<LIM, true, S>(w, f - 1, nt);
+        PR[v] = cell_edge<LIM, false, S + 1>(w, f, nt);
+    }
+    FaceOut<T> o;
+    if (SOLVER == HLLD_SOLVER_HLLD)
+        hlld_face<0, T, RB, double>(PL, PR, (T)p.gamma, false, o);
+    else
+        hlle_face<0, T>(PL, PR, (T)p.gamma, false, false, o);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        if (k != C_BX) p.F[k][fout] = o.F[k];
+}
+
 __device__ __forceinline__ unsigned long long block_max_any(unsigned long long x,
                                                             unsigned long long *sm) {
 #pragma unroll
@@ -900,7 +948,9 @@ __device__ __forceinline__ unsigned long long block_max_any(unsigned long long x
     return r;
 }
 
-template <int LIM, int SOLVER>
+// DRV = false: driver2d.rk_step on a ny = 1 grid; DRV = true: the 1D
+// driver's rk2_step (driver.py:192-236) and run loop (driver.py:388-412).
+template <int LIM, int SOLVER, bool DRV>
 __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
     __shared__ unsigned long long red[33];
     __shared__ int s_tube;
@@ -918,7 +968,7 @@ __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
         const int64_t fbase = base + ti;  // tube ti has nt + 1 faces
         const double dx = p.dx[ti];
         // conserved variables from the primitives (hlld.py:185-217)
-        for (int c = threadIdx.x; c < nt; c += blockDim.x) {
+        for (int c = threadIdx.x; c < nt && !p.resume; c += blockDim.x) {
             double Pd[NPRIM], Cd[NCONS];
 #pragma unroll
             for (int k = 0; k < NPRIM; ++k) Pd[k] = (double)p.P[k][base + c];
@@ -929,8 +979,8 @@ __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
         __syncthreads();
         double t = 0.0;
         int steps = 0;
-        const int nst = p.scheme == 3 ? 3 : 2;
-        while (t < p.tend - 1e-14 && steps < p.max_steps) {
+        const int nst = DRV ? 2 : (p.scheme == 3 ? 3 : 2);
+        while ((DRV ? t < p.tend : t < p.tend - 1e-14) && steps < p.max_steps) {
             // dt = (cfl dx) / max(|vx| + v_fast) over the physical cells
             unsigned long long mloc = 0;
             for (int c = ng + threadIdx.x; c < ng + L; c += blockDim.x) {
@@ -951,7 +1001,8 @@ __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
                 unsigned long long b = abs_bits(fabs(vx) + vf);
                 mloc = mloc > b ? mloc : b;
             }
-            const double mx = __longlong_as_double((long long)block_max_any(mloc, red));
+            double mx = __longlong_as_double((long long)block_max_any(mloc, red));
+            if (DRV && p.light) mx = 1.0;  // driver.py:120-125
             double dt = isnan(mx) ? mx : (1.0 / clamp_lo(mx, 1e-14)) * (p.cfl * dx);
             if (dt > p.tend - t) dt = p.tend - t;
             if (!(dt > 0.0)) break;
@@ -961,10 +1012,28 @@ __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
             for (int st = 0; st < nst; ++st) {
                 const double *w = p.scheme == 3 ? kRK3d[st] : kRK2d[st];
                 const double w2 = w[2] * dt;
-                for (int f = threadIdx.x; f <= nt; f += blockDim.x)
-                    tube_face<LIM, SOLVER>(p, base, nt, f, fbase + f);
+                if (DRV) {
+                    // physical faces ng .. ng + L (reconstruction.py:354-373)
+                    for (int f = ng + threadIdx.x; f <= ng + L; f += blockDim.x)
+                        tube_face_driver1d<LIM, SOLVER>(p, base, nt, f, fbase + f);
+                } else {
+                    for (int f = threadIdx.x; f <= nt; f += blockDim.x)
+                        tube_face<LIM, SOLVER>(p, base, nt, f, fbase + f);
+                }
                 __syncthreads();
-                for (int c = threadIdx.x; c < nt; c += blockDim.x) {
+                // Heun (driver.py:223-232): U1 = U + dt L(U); U' = 0.5 (U + U1 + dt L(U1)),
+                // with rhs = (F_c - F_c+1) / dx on the physical cells; Bx held
+                for (int c = ng + threadIdx.x; DRV && c < ng + L; c += blockDim.x) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        if (k == C_BX) continue;
+                        const double rhs = (double)((p.F[k][fbase + c] - p.F[k][fbase + c + 1]) / R(dx));
+                        const int64_t ci = base + c;
+                        p.U[k][ci] = st == 0 ? p.U0[k][ci] + dt * rhs
+                                             : 0.5 * (p.U0[k][ci] + p.U[k][ci] + dt * rhs);
+                    }
+                }
+                for (int c = threadIdx.x; !DRV && c < nt; c += blockDim.x) {
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
                         double rhs;
@@ -1270,12 +1339,15 @@ void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Sc
 }
 
 template <int LIM>
-static void launch_tubes_lim(int solver, const TubesParams &tp, int blocks, int threads,
+static void launch_tubes_lim(int solver, bool drv, const TubesParams &tp, int blocks, int threads,
                              cudaStream_t st) {
-    if (solver == HLLD_SOLVER_HLLD)
-        tubes_kernel<LIM, HLLD_SOLVER_HLLD><<<blocks, threads, 0, st>>>(tp);
-    else
-        tubes_kernel<LIM, HLLD_SOLVER_HLLE><<<blocks, threads, 0, st>>>(tp);
+    if (solver == HLLD_SOLVER_HLLD) {
+        if (drv) tubes_kernel<LIM, HLLD_SOLVER_HLLD, true><<<blocks, threads, 0, st>>>(tp);
+        else tubes_kernel<LIM, HLLD_SOLVER_HLLD, false><<<blocks, threads, 0, st>>>(tp);
+    } else {
+        if (drv) tubes_kernel<LIM, HLLD_SOLVER_HLLE, true><<<blocks, threads, 0, st>>>(tp);
+        else tubes_kernel<LIM, HLLD_SOLVER_HLLE, false><<<blocks, threads, 0, st>>>(tp);
+    }
 }
 
 void launch_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
@@ -1286,6 +1358,9 @@ void launch_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *pri
     tp.ng = b->ng;
     tp.max_steps = b->max_steps;
     tp.scheme = b->scheme;
+    tp.light = b->flavor == HLLD_TUBE_DRIVER1D_LIGHT;
+    tp.resume = b->resume;
+    const bool drv = b->flavor != HLLD_TUBE_RK_STEP;
     tp.ncells = b->ncells;
     tp.cell_off = b->cell_off;
     tp.dx = b->dx;
@@ -1305,12 +1380,12 @@ void launch_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *pri
     tp.next = next;
     cudaMemsetAsync(next, 0, sizeof(unsigned int), st);
     switch (b->limiter) {
-    case HLLD_LIM_PCM: launch_tubes_lim<HLLD_LIM_PCM>(b->solver, tp, blocks, threads, st); break;
-    case HLLD_LIM_MC: launch_tubes_lim<HLLD_LIM_MC>(b->solver, tp, blocks, threads, st); break;
-    case HLLD_LIM_MINMOD: launch_tubes_lim<HLLD_LIM_MINMOD>(b->solver, tp, blocks, threads, st); break;
-    case HLLD_LIM_WENO5Z: launch_tubes_lim<HLLD_LIM_WENO5Z>(b->solver, tp, blocks, threads, st); break;
-    case HLLD_LIM_MP5: launch_tubes_lim<HLLD_LIM_MP5>(b->solver, tp, blocks, threads, st); break;
-    default: launch_tubes_lim<HLLD_LIM_MP7>(b->solver, tp, blocks, threads, st); break;
+    case HLLD_LIM_PCM: launch_tubes_lim<HLLD_LIM_PCM>(b->solver, drv, tp, blocks, threads, st); break;
+    case HLLD_LIM_MC: launch_tubes_lim<HLLD_LIM_MC>(b->solver, drv, tp, blocks, threads, st); break;
+    case HLLD_LIM_MINMOD: launch_tubes_lim<HLLD_LIM_MINMOD>(b->solver, drv, tp, blocks, threads, st); break;
+    case HLLD_LIM_WENO5Z: launch_tubes_lim<HLLD_LIM_WENO5Z>(b->solver, drv, tp, blocks, threads, st); break;
+    case HLLD_LIM_MP5: launch_tubes_lim<HLLD_LIM_MP5>(b->solver, drv, tp, blocks, threads, st); break;
+    default: launch_tubes_lim<HLLD_LIM_MP7>(b->solver, drv, tp, blocks, threads, st); break;
     }
 }
 

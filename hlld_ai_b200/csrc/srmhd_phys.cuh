@@ -50,7 +50,7 @@ template <> struct K<float> {
     static constexpr float tiny = 1e-30f;
     static constexpr float c2p_tol = 1e-6f;
     static constexpr float pstar_tol = 1e-5f;
-    static constexpr float weno_eps = 1e-30f;
+    static constexpr float weno_eps = 1e-20f;  // tau5 / eps stays finite for tau5 < 3e18
     static constexpr float mp_eps = 1e-30f;
     static constexpr float safe_df = 1e-30f;
     static constexpr int mu_plus_iters = 24;

@@ -29,6 +29,8 @@ from .physics.state import PRIM_KEYS
 
 
 TubesC = _lib.TubesC
+FLAVORS = {"rk_step": _lib.TUBE_RK_STEP, "driver1d_light": _lib.TUBE_DRIVER1D_LIGHT,
+           "driver1d_cfl": _lib.TUBE_DRIVER1D_CFL}
 
 
 @dataclass
@@ -82,16 +84,20 @@ class TubeBatch:
 
     def __init__(self, states: TubeStates, *, limiter: str = "weno5z", solver: str = "hlld",
                  scheme: str = "rk3", precision: str = "fp64", gamma: float = 5.0 / 3.0,
-                 atmo_rho: float = 1e-10, device="cuda"):
+                 atmo_rho: float = 1e-10, device="cuda", flavor: str = "rk_step",
+                 ng: int | None = None):
         from .physics.reconstruction import ghosts_needed
 
         if precision not in ("fp64", "fp64_exact", "mixed"):
             raise ValueError(f"unknown precision {precision!r}")
+        if flavor not in FLAVORS:
+            raise ValueError(f"unknown flavor {flavor!r}")
+        self.flavor = flavor
         self.states = states
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise TypeError("tubes run on a CUDA device only")
-        self.ng = ghosts_needed(limiter)
+        self.ng = ghosts_needed(limiter) if ng is None else int(ng)
         self.limiter, self.solver, self.scheme, self.precision = limiter, solver, scheme, precision
         self.gamma, self.atmo_rho = gamma, atmo_rho
         n = len(states.lengths)
@@ -130,17 +136,24 @@ class TubeBatch:
         for k in PRIM_KEYS:
             self.prims[k].copy_(torch.as_tensor(self.host_init[k], dtype=self.pdtype))
 
-    def _c(self, tend: float, cfl: float, max_steps: int) -> TubesC:
+    def _c(self, tend: float, cfl: float, max_steps: int, resume: bool) -> TubesC:
         return TubesC(self.n, self.ng, self.ncells.data_ptr(), self.cell_off.data_ptr(),
                       self.dx.data_ptr(), self.order.data_ptr(), float(cfl), float(tend),
                       int(max_steps), _lib.LIMITERS[self.limiter], _lib.SOLVERS[self.solver],
                       3 if self.scheme == "rk3" else 2, _lib.PRECISIONS[self.precision],
-                      float(self.gamma), float(self.atmo_rho))
+                      float(self.gamma), float(self.atmo_rho), FLAVORS[self.flavor],
+                      int(bool(resume)))
 
     def launch(self, tend: float, cfl: float = 0.4, max_steps: int = 1 << 30,
-               threads: int | None = None, blocks: int | None = None) -> None:
-        """Enqueue one persistent launch that advances every tube to tend."""
-        self._cdesc = self._c(tend, cfl, max_steps)  # kept alive for graph replays
+               threads: int | None = None, blocks: int | None = None,
+               resume: bool = False) -> None:
+        """Enqueue one persistent launch that advances every tube by tend
+        (from t = 0 of this launch).  resume=False rebuilds the conserved
+        state from the primitives first; resume=True continues from the
+        conserved state the previous launch left (a run split into
+        chunks then equals one run, apart from the step cut at each chunk
+        end)."""
+        self._cdesc = self._c(tend, cfl, max_steps, resume)  # kept alive for graph replays
         with torch.cuda.device(self.device):
             rc = _lib.lib().hlld_tubes_run(
                 ctypes.byref(self._cdesc), _lib.ptr_array(self.cons),
@@ -150,15 +163,17 @@ class TubeBatch:
                 int(blocks if blocks is not None else self.blocks), _lib.stream_handle(self.device))
         _lib.check(rc, "hlld_tubes_run")
 
-    def capture(self, tend: float, cfl: float = 0.4, max_steps: int = 1 << 30) -> torch.cuda.CUDAGraph:
-        """Capture the launch in a CUDA graph (replay advances the tubes from
-        whatever primitives they hold)."""
+    def capture(self, tend: float, cfl: float = 0.4, max_steps: int = 1 << 30,
+                resume: bool = False) -> torch.cuda.CUDAGraph:
+        """Capture the launch in a CUDA graph (each replay advances the tubes
+        by tend from the primitives -- or, with resume, the conserved state
+        -- they hold)."""
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream(self.device)
         s.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(s):
             with torch.cuda.graph(g, stream=s):
-                self.launch(tend, cfl, max_steps)
+                self.launch(tend, cfl, max_steps, resume=resume)
         torch.cuda.current_stream(self.device).wait_stream(s)
         self._graph = g
         return g
@@ -166,6 +181,14 @@ class TubeBatch:
     def cell_updates(self) -> int:
         """Physical cell-updates (cells x steps) of the last run."""
         return int((self.steps_out.to(torch.int64).cpu() * torch.as_tensor(self.states.lengths)).sum())
+
+    def tube_cons(self, i: int) -> dict:
+        """Conserved variables of tube i (ghosts included), float64 numpy."""
+        from .physics.state import CONS_KEYS
+
+        a = int(self.cell_off[i].item())
+        b = a + int(self.states.lengths[i]) + 2 * self.ng
+        return {k: self.cons[j][a:b].cpu().numpy() for j, k in enumerate(CONS_KEYS)}
 
     def tube(self, i: int) -> dict:
         """Primitives of tube i (ghosts included), as float64 numpy."""
@@ -183,7 +206,7 @@ class TubeBatch:
                          {k: v[idx] for k, v in self.states.right.items()}, self.states.Bx[idx])
         probe = TubeBatch(sub, limiter=self.limiter, solver=self.solver, scheme=self.scheme,
                           precision=self.precision, gamma=self.gamma, atmo_rho=self.atmo_rho,
-                          device=self.device)
+                          device=self.device, flavor=self.flavor, ng=self.ng)
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         best = None
         for threads, per_sm in shapes:

@@ -107,12 +107,33 @@ typedef struct {
     void *prims[9];
 } hlld_state2d_t;
 
+/* How each tube of a batch is stepped (hlld_tubes_t.flavor). */
+enum hlld_tube_flavor {
+    /* src/physics/driver2d.py:309-355 rk_step on a ny = 1 grid: W v
+     * reconstruction with the PCM positivity fallback, SSP-RK2/3 per
+     * `scheme`, dt = compute_dt (driver.py:77-127) with the fast speed,
+     * stepping while t < tend - 1e-14 */
+    HLLD_TUBE_RK_STEP = 0,
+    /* src/physics/driver.py:130-236 compute_rhs + rk2_step (the 1D
+     * shock-tube driver): all nine primitives reconstructed as they are,
+     * Heun RK2 with Bx held, dt = cfl dx (compute_dt with speed_of_light,
+     * the driver's default, driver.py:390), stepping while t < tend */
+    HLLD_TUBE_DRIVER1D_LIGHT = 1,
+    /* as HLLD_TUBE_DRIVER1D_LIGHT with the fast-speed compute_dt
+     * (run.dt_speed_of_light = false) */
+    HLLD_TUBE_DRIVER1D_CFL = 2
+};
+
 /* A batch of independent 1D tubes (the batched-tube workload): tube i has
  * ncells[i] physical cells and ng ghosts per side, occupies cells
  * cell_off[i] .. cell_off[i] + ncells[i] + 2 ng - 1 of the concatenated cell
  * arrays and faces cell_off[i] + i .. cell_off[i] + i + ncells[i] + 2 ng of
  * the face arrays, and has cell width dx[i].  order (may be NULL) is the
- * processing order (e.g. longest tube first).  All pointers are device. */
+ * processing order (e.g. longest tube first).  All pointers are device.
+ * resume = 0: the conserved arrays are first computed from the primitives
+ * (a fresh run); resume = 1: cons already holds the state that goes with
+ * the primitives (a continued run, or the reference's rk2_step, which takes
+ * both). */
 typedef struct {
     int32_t ntubes, ng;
     const int32_t *ncells;
@@ -123,6 +144,8 @@ typedef struct {
     int32_t max_steps;
     int32_t limiter, solver, scheme, precision;
     double gamma, atmo_rho;
+    int32_t flavor;       /* enum hlld_tube_flavor */
+    int32_t resume;
 } hlld_tubes_t;
 
 int hlld_version(void);
@@ -213,7 +236,9 @@ int hlld_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *cons
  * workload, with a dt per tube: every tube runs src/physics/driver2d.py:309-355
  * rk_step on a ny = 1 grid (x sweep only -- the y sweep of a ny = 1 grid
  * contributes exactly zero), dt from src/physics/driver.py:77-127
- * compute_dt each step, until tend or max_steps, in ONE persistent launch of
+ * compute_dt each step, until tend or max_steps (flavor HLLD_TUBE_RK_STEP),
+ * or the 1D driver's loop (src/physics/driver.py:388-412 around rk2_step,
+ * the other flavors), in ONE persistent launch of
  * `blocks` CTAs of `threads` threads (0 = library defaults).  prims (9
  * arrays, ghosts filled) are read and updated in place; cons (8), U0 (8
  * cell arrays) and F (8 face arrays, slot Bx unused) are work arrays;

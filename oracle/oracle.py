@@ -244,3 +244,27 @@ def tube_run(prims: dict, L: int, ng: int, dx: float, cfl: float, tend: float, l
                                ctypes.c_double(atmo_rho), ctypes.c_int(3 if scheme == "rk3" else 2),
                                P, ctypes.byref(t))
     return t.value, int(steps)
+
+
+TUBE_FLAVORS = {"rk_step": 0, "driver1d_light": 1, "driver1d_cfl": 2}
+
+
+def tube_run_ex(prims: dict, L: int, ng: int, dx: float, cfl: float, tend: float, limiter: str,
+                solver: str, gamma: float, *, scheme: str = "rk3", flavor: str = "rk_step",
+                cons: dict | None = None, resume: bool = False, max_steps: int = 1 << 30,
+                atmo_rho: float = 1e-10):
+    """orc_tube_run_ex: one tube in the given stepping flavor, in place on 9
+    primitive arrays (and the 8 conserved arrays when given; with
+    resume=True they are the starting state); returns (t, steps)."""
+    P = _ptrs([prims[k] for k in PRIM_KEYS])
+    C = _ptrs([cons[k] for k in CONS_KEYS]) if cons is not None else None
+    t = ctypes.c_double(0.0)
+    steps = lib().orc_tube_run_ex(ctypes.c_int(L), ctypes.c_int(ng), ctypes.c_double(dx),
+                                  ctypes.c_double(cfl), ctypes.c_double(tend),
+                                  ctypes.c_int(max_steps), ctypes.c_int(LIMITERS[limiter]),
+                                  ctypes.c_int(SOLVERS[solver]), ctypes.c_double(gamma),
+                                  ctypes.c_double(atmo_rho),
+                                  ctypes.c_int(3 if scheme == "rk3" else 2),
+                                  ctypes.c_int(TUBE_FLAVORS[flavor]), ctypes.c_int(int(resume)),
+                                  C, P, ctypes.byref(t))
+    return t.value, int(steps)

@@ -1528,10 +1528,48 @@ static double tube_dt(int L, int ng, double dx, double cfl, double gamma,
     return (1.0 / mx) * (cfl * dx);
 }
 
+/* driver.py:388-412: the 1D driver's loop around rk2_step; dt from
+ * compute_dt (speed_of_light -> max speed 1, i.e. (1/1) (cfl dx)) */
+static int driver1d_run(int L, int ng, double dx, double cfl, double tend, int max_steps,
+                        int limiter, int solver, double gamma, double atmo_rho, int light,
+                        double *const *cons, double *const *prim, double *t_out) {
+    double t = 0.0;
+    int steps = 0;
+    while (t < tend && steps < max_steps) {
+        double dt = light ? (1.0 / 1.0) * (cfl * dx)
+                          : tube_dt(L, ng, dx, cfl, gamma, (const double *const *)prim);
+        if (dt > tend - t) dt = tend - t;
+        if (!(dt > 0.0)) break;
+        orc_rk2_step_1d(L, ng, dx, dt, limiter, solver, gamma, atmo_rho, cons, prim);
+        t += dt;
+        steps++;
+    }
+    if (t_out) *t_out = t;
+    return steps;
+}
+
 int orc_tube_run(int L, int ng, double dx, double cfl, double tend, int max_steps, int limiter,
                  int solver, double gamma, double atmo_rho, int scheme, double *const *prim,
                  double *t_out) {
+    return orc_tube_run_ex(L, ng, dx, cfl, tend, max_steps, limiter, solver, gamma, atmo_rho,
+                           scheme, ORC_TUBE_RK_STEP, 0, NULL, prim, t_out);
+}
+
+int orc_tube_run_ex(int L, int ng, double dx, double cfl, double tend, int max_steps, int limiter,
+                    int solver, double gamma, double atmo_rho, int scheme, int flavor, int resume,
+                    double *const *cons, double *const *prim, double *t_out) {
     const int nt = L + 2 * ng, nf = nt + 1;
+    if (flavor != ORC_TUBE_RK_STEP) {
+        double *C[ORC_NCONS];
+        for (int k = 0; k < ORC_NCONS; ++k)
+            C[k] = cons ? cons[k] : (double *)malloc(sizeof(double) * nt);
+        if (!resume) orc_prim_to_cons(nt, (const double *const *)prim, C);
+        int steps = driver1d_run(L, ng, dx, cfl, tend, max_steps, limiter, solver, gamma, atmo_rho,
+                                 flavor == ORC_TUBE_DRIVER1D_LIGHT, C, prim, t_out);
+        if (!cons)
+            for (int k = 0; k < ORC_NCONS; ++k) free(C[k]);
+        return steps;
+    }
     const double(*tab)[3] = scheme == 3 ? RK3 : RK2;
     const int nst = scheme == 3 ? 3 : 2;
     double *U[ORC_NCONS], *U0[ORC_NCONS], *F[ORC_NCONS], *Uf[ORC_NCONS];
@@ -1547,7 +1585,10 @@ int orc_tube_run(int L, int ng, double dx, double cfl, double tend, int max_step
         Rp[k] = (double *)malloc(sizeof(double) * nf);
     }
     double *ps = (double *)malloc(sizeof(double) * nf);
-    orc_prim_to_cons(nt, (const double *const *)prim, U);
+    if (resume && cons)
+        for (int k = 0; k < ORC_NCONS; ++k) memcpy(U[k], cons[k], sizeof(double) * nt);
+    else
+        orc_prim_to_cons(nt, (const double *const *)prim, U);
     double t = 0.0;
     int steps = 0;
     while (t < tend - 1e-14 && steps < max_steps) {
@@ -1578,6 +1619,8 @@ int orc_tube_run(int L, int ng, double dx, double cfl, double tend, int max_step
         steps++;
     }
     if (t_out) *t_out = t;
+    if (cons)
+        for (int k = 0; k < ORC_NCONS; ++k) memcpy(cons[k], U[k], sizeof(double) * nt);
     for (int k = 0; k < ORC_NCONS; ++k) {
         free(U[k]); free(U0[k]); free(F[k]); free(Uf[k]);
     }

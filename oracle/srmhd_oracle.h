@@ -145,6 +145,17 @@ int orc_tube_run(int L, int ng, double dx, double cfl, double tend, int max_step
                  int solver, double gamma, double atmo_rho, int scheme, double *const *prim,
                  double *t_out);
 
+/* The same with the stepping flavor and the conserved state exposed:
+ * flavor ORC_TUBE_RK_STEP is orc_tube_run; ORC_TUBE_DRIVER1D_LIGHT /
+ * ORC_TUBE_DRIVER1D_CFL run driver.py:388-412 (rk2_step = orc_rk2_step_1d
+ * each step, dt = cfl dx or compute_dt, while t < tend).  cons (8 arrays of
+ * L + 2 ng, may be NULL): with resume = 1 it is the starting conserved
+ * state (else it is computed from prim); on return it holds the final one. */
+enum { ORC_TUBE_RK_STEP = 0, ORC_TUBE_DRIVER1D_LIGHT = 1, ORC_TUBE_DRIVER1D_CFL = 2 };
+int orc_tube_run_ex(int L, int ng, double dx, double cfl, double tend, int max_steps, int limiter,
+                    int solver, double gamma, double atmo_rho, int scheme, int flavor, int resume,
+                    double *const *cons, double *const *prim, double *t_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -208,3 +208,31 @@ def test_tube_runs_match_reference(ti):
     assert abs(t - float(np.sum(z[f"t{ti}_dt"]))) <= 1e-12 * t
     for k in PK:
         assert max_rel(z[f"t{ti}_prims_{k}"], prims[k]) < 1e-11, k
+
+
+def test_driver_flavor_reproduces_the_reference_rk2_steps():
+    """The 1D driver loop (dt = cfl dx, speed-of-light compute_dt) for six
+    steps is the reference's six rk2_step calls of the Brio-Wu golden."""
+    z = load("tube1d.npz")
+    prims = {k: z[f"init_{k}"].copy() for k in PK}
+    t, steps = oracle.tube_run_ex(prims, 800, 2, 1.0 / 800, 0.4, 1.0, "mc", "hlld", 2.0,
+                                  flavor="driver1d_light", max_steps=6)
+    assert steps == 6 and abs(t - 6 * float(z["dt"])) < 1e-15
+    for k in PK:
+        assert max_rel(z[f"prims_{k}"], prims[k]) < 1e-11, k
+
+
+def test_tube_run_resumes_from_its_conserved_state():
+    """Two resumed runs of two steps each equal one run of four steps."""
+    z = load("tubes.npz")
+    L = int(z["t0_L"])
+    a = {k: z[f"t0_init_{k}"].copy() for k in PK}
+    b = {k: z[f"t0_init_{k}"].copy() for k in PK}
+    oracle.tube_run(a, L, 3, 1.0 / L, 0.4, 10.0, "weno5z", "hlld", 5.0 / 3.0, max_steps=4)
+    cons = {k: np.zeros(L + 6) for k in oracle.CONS_KEYS}
+    oracle.tube_run_ex(b, L, 3, 1.0 / L, 0.4, 10.0, "weno5z", "hlld", 5.0 / 3.0, cons=cons,
+                       max_steps=2)
+    oracle.tube_run_ex(b, L, 3, 1.0 / L, 0.4, 10.0, "weno5z", "hlld", 5.0 / 3.0, cons=cons,
+                       resume=True, max_steps=2)
+    for k in PK:
+        assert np.array_equal(a[k], b[k]), k
