@@ -300,6 +300,19 @@ def _l1_mixed_vs_fp64(a, dev, steps):
     return res
 
 
+# DRAM bytes (read + write) of one mixed-precision sweep launch measured by
+# ncu on the rotor at 1536^2 (x: 95.0 + 41.3 MB, y: 95.0 + 38.7 MB over
+# 2,373,140 faces), per face; the 2048^2 launch is scaled by its faces
+_SWEEP_DRAM_BYTES_PER_FACE_MIXED = (136.3e6 + 133.7e6) / 2 / 2373140
+
+
+def _sweep_traffic(a):
+    if a.precision != "mixed":
+        return None
+    nt = a.n + 4
+    return _SWEEP_DRAM_BYTES_PER_FACE_MIXED * (nt + 1) * nt
+
+
 def run_ours(a):
     import torch
     import torch.distributed as dist
@@ -412,7 +425,10 @@ def run_ours(a):
             "gpu_launches": launches_per_step * a.steps,
             "roofline": {"bound": "hbm", "kernel": "sweep_kernel (x and y)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": _sweep_traffic(a), "traffic_unit": "bytes per launch",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                           "of the mixed sweep at 1536^2, scaled by faces",
                          "bytes_per_face": bytes_per_face,
                          "avg_launch_ms": sweep_avg_s * 1e3, "share_of_step": sweep_share},
             "cpu_baseline": cpu,

