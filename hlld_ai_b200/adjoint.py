@@ -1,0 +1,275 @@
+"""Gradients through many RK+CT steps: the discrete adjoint on the GPU.
+
+``CheckpointedRun`` runs the FP64 2D step forward for a fixed sequence of
+time steps, keeping the state every ``checkpoint_every`` steps, and runs the
+adjoint backward: each segment is recomputed from its checkpoint (all its
+step states kept), then the steps are reversed one by one with
+``hlld_adjoint_rk_step_ct``, the transpose of the step's Jacobian with the
+time step fixed and every discrete decision frozen at its forward outcome
+(limiter branches, HLLD region and fallback, CT upwind signs); the HLLD p*
+and the Kastaun C2P root are differentiated by the implicit-function
+theorem.  The reference has no adjoint; its gradients would come from torch
+autograd through ``src/physics/driver2d.py:420-448`` rk_step_ct, which the
+same step sequence reproduces.
+
+``RKSteps`` wraps a run in a ``torch.autograd.Function`` over the conserved
+state (the six evolved cell variables and the two face fields), so a torch
+objective of the final state backpropagates into the initial state.
+``rotor_gradients`` is the magnetic-rotor study: the gradient of the
+Gaussian-weighted final magnetic energy with respect to the initial density
+field and the rotor's angular velocity.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib
+from .physics.driver2d import Stepper2D
+from .physics.state import CONS_KEYS, EVOLVED_KEYS, PRIM_KEYS, State2D
+
+_SCHEMES = {"rk2": 2, "rk3": 3}
+
+
+def _zeros_state(grid, device) -> State2D:
+    z = lambda *s: torch.zeros(*s, dtype=torch.float64, device=device)
+    return State2D(cons={k: z(grid.nxt, grid.nyt) for k in EVOLVED_KEYS},
+                   Bxf=z(grid.nxt + 1, grid.nyt), Byf=z(grid.nxt, grid.nyt + 1),
+                   prims={k: z(grid.nxt, grid.nyt) for k in PRIM_KEYS})
+
+
+class CheckpointedRun:
+    """Forward steps with checkpoints, and the adjoint of the whole run."""
+
+    def __init__(self, grid, eos, *, bc_x="periodic", bc_y="periodic", flux_fn="hlld",
+                 limiter="mc", scheme="rk3", upwind=True, atmo_rho=1e-10,
+                 checkpoint_every=20):
+        if checkpoint_every < 1:
+            raise ValueError("checkpoint_every must be >= 1")
+        self.grid, self.eos, self.scheme = grid, eos, scheme
+        self.every = int(checkpoint_every)
+        self.stepper = Stepper2D(grid, eos, bc_x=bc_x, bc_y=bc_y, flux_fn=flux_fn,
+                                 limiter=limiter, upwind=upwind, atmo_rho=atmo_rho,
+                                 precision="fp64")
+        self.device = self.stepper.device
+        n = ctypes.c_size_t(0)
+        _lib.check(_lib.lib().hlld_adjoint_scratch_bytes(ctypes.byref(self.stepper.gc),
+                                                         ctypes.byref(n)),
+                   "hlld_adjoint_scratch_bytes")
+        self._scratch = torch.empty(n.value + 256, dtype=torch.uint8, device=self.device)
+        self._scratch_ptr = (self._scratch.data_ptr() + 255) // 256 * 256
+        self._scratch_bytes = n.value
+        self.checkpoints: list[State2D] = []
+        self.dts: list[float] = []
+
+    # -- forward ----------------------------------------------------------
+    def forward(self, state: State2D, dts) -> State2D:
+        """Advance a copy of the (synced, FP64) state through dts; returns
+        the final state and keeps the checkpoints."""
+        self.dts = [float(d) for d in dts]
+        s = state.clone()
+        self.checkpoints = []
+        for i, dt in enumerate(self.dts):
+            if i % self.every == 0:
+                self.checkpoints.append(s.clone())
+            self.stepper.step(s, dt, self.scheme)
+        self.final = s
+        return s
+
+    def step_adjoint(self, s_in: State2D, s_out: State2D, dt: float, lam: State2D) -> None:
+        """lam: gradient with respect to s_out -> gradient with respect to s_in (in place)."""
+        st = self.stepper
+        a, b, l = st._struct(s_in), st._struct(s_out), st._struct(lam)
+        with torch.cuda.device(self.device):
+            rc = _lib.lib().hlld_adjoint_rk_step_ct(
+                ctypes.byref(st.gc), ctypes.byref(a), ctypes.byref(b), float(dt),
+                _SCHEMES[self.scheme], ctypes.byref(l), self._scratch_ptr, self._scratch_bytes,
+                _lib.stream_handle(self.device))
+        _lib.check(rc, "hlld_adjoint_rk_step_ct")
+
+    # -- backward ---------------------------------------------------------
+    def backward(self, lam: State2D) -> State2D:
+        """lam: gradient of the objective with respect to the final state
+        (cons, faces and prims; missing prims are zero).  Returns the
+        gradient with respect to the initial state's cons and faces."""
+        lam = State2D(cons={k: lam.cons[k].clone() for k in EVOLVED_KEYS}, Bxf=lam.Bxf.clone(),
+                      Byf=lam.Byf.clone(),
+                      prims={k: (lam.prims[k].clone() if k in lam.prims else
+                                 torch.zeros_like(lam.cons["D"])) for k in PRIM_KEYS})
+        nsteps = len(self.dts)
+        for seg in range(len(self.checkpoints) - 1, -1, -1):
+            i0 = seg * self.every
+            i1 = min(i0 + self.every, nsteps)
+            states = [self.checkpoints[seg].clone()]
+            for i in range(i0, i1):
+                s = states[-1].clone()
+                self.stepper.step(s, self.dts[i], self.scheme)
+                states.append(s)
+            for i in range(i1 - 1, i0 - 1, -1):
+                self.step_adjoint(states[i - i0], states[i - i0 + 1], self.dts[i], lam)
+            del states
+        return lam
+
+
+class RKSteps(torch.autograd.Function):
+    """Final conserved state of a CheckpointedRun as a differentiable
+    function of the initial one: inputs and outputs are the six evolved cell
+    variables then Bxf and Byf."""
+
+    @staticmethod
+    def forward(ctx, run: CheckpointedRun, dts, *cons_faces):
+        g = run.grid
+        s = State2D(cons={k: cons_faces[i].detach().clone().contiguous()
+                          for i, k in enumerate(EVOLVED_KEYS)},
+                    Bxf=cons_faces[6].detach().clone().contiguous(),
+                    Byf=cons_faces[7].detach().clone().contiguous(), prims={})
+        run.stepper.sync(s)
+        out = run.forward(s, dts)
+        ctx.run = run
+        return tuple([out.cons[k].clone() for k in EVOLVED_KEYS] + [out.Bxf.clone(), out.Byf.clone()])
+
+    @staticmethod
+    def backward(ctx, *grads):
+        run = ctx.run
+        g = run.grid
+        lam = _zeros_state(g, run.device)
+        for i, k in enumerate(EVOLVED_KEYS):
+            if grads[i] is not None:
+                lam.cons[k].copy_(grads[i])
+        if grads[6] is not None:
+            lam.Bxf.copy_(grads[6])
+        if grads[7] is not None:
+            lam.Byf.copy_(grads[7])
+        lam0 = run.backward(lam)
+        return (None, None, *[lam0.cons[k] for k in EVOLVED_KEYS], lam0.Bxf, lam0.Byf)
+
+
+def prim_to_cons_vjp(prims: dict, lam_cons: dict) -> dict:
+    """(d cons / d prims)^T lam_cons per cell (hlld.py:185-217 in reverse);
+    prims: the nine FP64 primitive arrays; lam_cons: any of the eight
+    conserved keys (missing ones are zero).  Returns the nine lambdas."""
+    ref = prims["rho"]
+    n = ref.numel()
+    P = [prims[k].contiguous() for k in PRIM_KEYS]
+    lc = [lam_cons[k].contiguous() if k in lam_cons else None for k in CONS_KEYS]
+    out = {k: torch.empty_like(ref) for k in PRIM_KEYS}
+    lc_ptrs = (ctypes.c_void_p * 8)(*[t.data_ptr() if t is not None else None for t in lc])
+    with torch.cuda.device(ref.device):
+        rc = _lib.lib().hlld_prim_to_cons_vjp(n, _lib.ptr_array(P), lc_ptrs,
+                                              _lib.ptr_array([out[k] for k in PRIM_KEYS]),
+                                              _lib.stream_handle(ref.device))
+    _lib.check(rc, "hlld_prim_to_cons_vjp")
+    return out
+
+
+# ── the magnetic-rotor gradient study ─────────────────────────────────────
+
+def gaussian_weight(grid, centre=(0.6, 0.5), sigma=0.1):
+    X, Y = grid.X, grid.Y
+    return torch.exp(-((X - centre[0]) ** 2 + (Y - centre[1]) ** 2) / (2.0 * sigma ** 2))
+
+
+def magnetic_objective(grid, weight, Bxf, Byf, Bz):
+    """J = sum over physical cells of w |B_c|^2 / 2, B_c the cell-centred
+    field (face averages for Bx, By; the cell Bz)."""
+    ph = grid.phys
+    Bcx = 0.5 * (Bxf[:-1, :] + Bxf[1:, :])
+    Bcy = 0.5 * (Byf[:, :-1] + Byf[:, 1:])
+    e = 0.5 * (Bcx ** 2 + Bcy ** 2 + Bz ** 2)
+    return (weight[ph] * e[ph]).sum()
+
+
+@dataclass
+class RotorCase:
+    n: int = 512
+    steps: int = 200
+    checkpoint_every: int = 20
+    omega: float = 9.95
+    cfl: float = 0.4
+
+
+def rotor_initial(grid, eos, rho0_phys, omega):
+    """Rotor primitives with the physical cells' density replaced by
+    rho0_phys (ghosts from the periodic images) and angular velocity omega,
+    and their conserved state, synced."""
+    from .physics.initial_data2d import b_from_potential, rotor_tapered
+
+    prims, Az = rotor_tapered(grid, eos, omega=omega)
+    prims = {k: v.to(torch.float64).contiguous() for k, v in prims.items()}
+    if rho0_phys is not None:
+        rho = prims["rho"].clone()
+        rho[grid.phys] = rho0_phys
+        prims["rho"] = rho
+        prims["eps"] = eos.eps__press_rho(prims["p"], prims["rho"])
+    Bxf, Byf = b_from_potential(Az, grid.dx, grid.dy)
+    return prims, Bxf.contiguous(), Byf.contiguous()
+
+
+def _cons_from(prims, grid):
+    from .physics.driver2d import prims_to_cons_2d
+
+    c = prims_to_cons_2d(prims, grid, "fp64")
+    return {k: c[k].contiguous() for k in EVOLVED_KEYS}
+
+
+def rotor_forward(run: CheckpointedRun, grid, eos, rho0_phys, omega, dts, weight):
+    """J of the rotor with the given density field and omega, the dt
+    sequence fixed."""
+    prims, Bxf, Byf = rotor_initial(grid, eos, rho0_phys, omega)
+    s = State2D(cons=_cons_from(prims, grid), Bxf=Bxf, Byf=Byf, prims={})
+    run.stepper.sync(s)
+    out = run.forward(s, dts)
+    return float(magnetic_objective(grid, weight, out.Bxf, out.Byf, out.cons["Bz"]))
+
+
+def rotor_gradients(case: RotorCase, device="cuda"):
+    """Forward + adjoint of the rotor study; returns J, dJ/d rho0 (physical
+    cells), dJ/d omega, the dt sequence and timings (CUDA events)."""
+    from .physics.eos import hybrid_eos
+    from .physics.grid import Grid2D
+
+    eos = hybrid_eos(K=0.0, gamma=5.0 / 3.0, gamma_th=5.0 / 3.0)
+    grid = Grid2D(0.0, 1.0, case.n, 0.0, 1.0, case.n, ng=2, device=device)
+    run = CheckpointedRun(grid, eos, bc_x="periodic", bc_y="periodic", limiter="mc",
+                          checkpoint_every=case.checkpoint_every)
+    weight = gaussian_weight(grid)
+    prims, Bxf, Byf = rotor_initial(grid, eos, None, case.omega)
+    s0 = State2D(cons=_cons_from(prims, grid), Bxf=Bxf, Byf=Byf, prims={})
+    run.stepper.sync(s0)
+    # the dt sequence of the unperturbed run (frozen for the gradient)
+    s = s0.clone()
+    dts = []
+    for _ in range(case.steps):
+        dt = float(run.stepper.compute_dt(s, case.cfl).item())
+        dts.append(dt)
+        run.stepper.step(s, dt, "rk3")
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    out = run.forward(s0, dts)
+    e1.record()
+    Bxf_o = out.Bxf.clone().requires_grad_(True)
+    Byf_o = out.Byf.clone().requires_grad_(True)
+    Bz_o = out.cons["Bz"].clone().requires_grad_(True)
+    J = magnetic_objective(grid, weight, Bxf_o, Byf_o, Bz_o)
+    J.backward()
+    lam = _zeros_state(grid, run.device)
+    lam.Bxf.copy_(Bxf_o.grad)
+    lam.Byf.copy_(Byf_o.grad)
+    lam.cons["Bz"].copy_(Bz_o.grad)
+    lam0 = run.backward(lam)
+    e2.record()
+    torch.cuda.synchronize()
+    # initial data: cons0 = P2C(prims0(rho0, omega)); eps = p / (rho (gamma - 1))
+    lp = prim_to_cons_vjp(prims, {k: lam0.cons[k] for k in EVOLVED_KEYS})
+    g_rho = lp["rho"] - lp["eps"] * prims["eps"] / prims["rho"]
+    ph = grid.phys
+    v_over_w = {k: prims[k] / case.omega for k in ("vx", "vy")}
+    g_omega = float((lp["vx"][ph] * v_over_w["vx"][ph] + lp["vy"][ph] * v_over_w["vy"][ph]).sum())
+    return {"J": float(J), "grad_rho0": g_rho[ph].contiguous(), "grad_omega": g_omega,
+            "dts": dts, "run": run, "grid": grid, "eos": eos, "weight": weight,
+            "forward_ms": e0.elapsed_time(e1), "adjoint_ms": e1.elapsed_time(e2),
+            "rho0": prims["rho"][ph].clone()}

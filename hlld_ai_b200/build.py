@@ -29,6 +29,7 @@ UNITS = [
     ("variant_exact.cu", ["-fmad=false"]),
     ("variant_mixed.cu", ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("noalloc.cu", []),
+    ("adjoint_fp64.cu", []),
 ]
 
 

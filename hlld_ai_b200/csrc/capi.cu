@@ -338,4 +338,46 @@ int hlld_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double c
     return check_launch("compute_dt_2d");
 }
 
+int hlld_prim_to_cons_vjp(int64_t n, const void *const *prim, const void *const *lam_cons,
+                          void *const *lam_prim, void *stream) {
+    if (n < 0) return fail(HLLD_ERR_INVALID, "n < 0");
+    if (n == 0) return HLLD_OK;
+    if (!prim || !lam_cons || !lam_prim) return fail(HLLD_ERR_INVALID, "NULL array argument");
+    for (int k = 0; k < 9; ++k)
+        if (!prim[k] || !lam_prim[k]) return fail(HLLD_ERR_INVALID, "prim / lam_prim[%d] is NULL", k);
+    hlld::v_adj::launch_prim_to_cons_vjp(n, prim, lam_cons, lam_prim, (cudaStream_t)stream);
+    return check_launch("prim_to_cons_vjp");
+}
+
+int hlld_adjoint_scratch_bytes(const hlld_grid2d_t *g, size_t *bytes) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (!bytes) return fail(HLLD_ERR_INVALID, "bytes is NULL");
+    if (g->precision != HLLD_FP64)
+        return fail(HLLD_ERR_UNSUPPORTED, "the adjoint is implemented for HLLD_FP64");
+    *bytes = hlld::v_adj::adjoint_scratch_bytes(g);
+    return HLLD_OK;
+}
+
+int hlld_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
+                            const hlld_state2d_t *s_out, double dt, int scheme,
+                            const hlld_state2d_t *lam, void *scratch, size_t scratch_bytes,
+                            void *stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (g->precision != HLLD_FP64)
+        return fail(HLLD_ERR_UNSUPPORTED, "the adjoint is implemented for HLLD_FP64");
+    if ((rc = check_state(s_in)) || (rc = check_state(s_out)) || (rc = check_state(lam))) return rc;
+    if (scheme != 2 && scheme != 3) return fail(HLLD_ERR_INVALID, "scheme must be 2 or 3");
+    if (!(dt > 0.0)) return fail(HLLD_ERR_INVALID, "dt must be > 0");
+    if (!scratch) return fail(HLLD_ERR_INVALID, "scratch is NULL");
+    if ((uintptr_t)scratch % kAlign) return fail(HLLD_ERR_INVALID, "scratch must be 256-byte aligned");
+    const size_t need = hlld::v_adj::adjoint_scratch_bytes(g);
+    if (scratch_bytes < need)
+        return fail(HLLD_ERR_SCRATCH, "scratch has %zu bytes, the adjoint needs %zu", scratch_bytes, need);
+    hlld::v_adj::launch_adjoint_rk_step_ct(g, s_in, s_out, dt, scheme, lam, scratch,
+                                             (cudaStream_t)stream);
+    return check_launch("adjoint_rk_step_ct");
+}
+
 }  // extern "C"

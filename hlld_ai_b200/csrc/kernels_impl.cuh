@@ -1085,6 +1085,9 @@ __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
 }
 
 // ── host-side launchers of this variant ──────────────────────────────────
+// (HLLD_DEVICE_ONLY: a translation unit that needs only the device code and
+// calls another unit's launchers)
+#ifndef HLLD_DEVICE_ONLY
 
 static inline unsigned grid1d(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
@@ -1400,6 +1403,8 @@ void launch_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, doubl
     speed_kernel<<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(sp);
     dt_kernel<<<1, 1, 0, st>>>(work, g->dx, g->dy, cfl, dt_dev);
 }
+
+#endif  // HLLD_DEVICE_ONLY
 
 }  // namespace HLLD_NS
 }  // namespace hlld

@@ -53,6 +53,14 @@ struct Scratch2D {
 int report_error(int code, const char *fmt, ...);
 
 HLLD_DECLARE_VARIANT(v_fp64)
+namespace v_adj {  // the discrete adjoint of the FP64 step (adjoint_fp64.cu)
+size_t adjoint_scratch_bytes(const hlld_grid2d_t *g);
+void launch_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
+                               const hlld_state2d_t *s_out, double dt, int scheme,
+                               const hlld_state2d_t *lam, void *scratch, cudaStream_t st);
+void launch_prim_to_cons_vjp(int64_t n, const void *const *prim, const void *const *lam_cons,
+                             void *const *lam_prim, cudaStream_t st);
+}
 HLLD_DECLARE_VARIANT(v_exact)
 HLLD_DECLARE_VARIANT(v_mixed)
 

@@ -249,6 +249,35 @@ int hlld_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
                    void *const *U0, void *const *F, double *t_out, int32_t *steps_out,
                    unsigned int *next, int threads, int blocks, void *stream);
 
+/* Reverse of src/physics/hlld.py:185-217 primitive_to_conserved on n
+ * elements (FP64): lam_prim[9] = (d cons / d prim)^T lam_cons[8], with eps
+ * an independent input as it is there.  Entries of lam_cons may be NULL
+ * (zero).  For gradients of an objective with respect to initial data. */
+int hlld_prim_to_cons_vjp(int64_t n, const void *const *prim, const void *const *lam_cons,
+                          void *const *lam_prim, void *stream);
+
+/* Bytes of scratch hlld_adjoint_rk_step_ct needs for this grid (FP64 only). */
+int hlld_adjoint_scratch_bytes(const hlld_grid2d_t *g, size_t *bytes);
+
+/* Discrete adjoint of one hlld_rk_step_ct step.  No counterpart in the
+ * reference, whose gradients would come from torch autograd through
+ * src/physics/driver2d.py:420-448 rk_step_ct; this is that step's
+ * transpose with its dt held fixed.  s_in is the step's input state and
+ * s_out the output the forward step made from it with dt.  lam (device
+ * arrays shaped like a state: cons[6], Bxf, Byf, prims[9], double) holds
+ * on entry the gradient of the objective with respect to the output state
+ * and on return its gradient with respect to the input state's cons and
+ * faces (lam.prims returns zeroed: the input primitives are a function of
+ * them).  Discrete decisions (limiter branches, HLLD region and fallback,
+ * upwind signs, clamps) are frozen at their forward outcome; p* and the C2P
+ * root are differentiated by the implicit-function theorem.  g->precision
+ * must be HLLD_FP64; scratch (256-byte aligned) of
+ * hlld_adjoint_scratch_bytes bytes. */
+int hlld_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
+                            const hlld_state2d_t *s_out, double dt, int scheme,
+                            const hlld_state2d_t *lam, void *scratch, size_t scratch_bytes,
+                            void *stream);
+
 /* Replaces src/physics/driver2d.py:251-281 compute_dt_2d: writes
  * dt = cfl / (max(|vx|+cf)/dx + max(|vy|+cf)/dy) to dt_dev (device double);
  * work (device, >= 2 unsigned long long) holds the running maxima. */
