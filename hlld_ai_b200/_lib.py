@@ -16,7 +16,7 @@ LIB_PATH = os.environ.get("HLLD_B200_LIB") or os.path.join(HERE, "libhlld_b200.s
 HLLD_OK = 0
 FP64, FP64_EXACT, MIXED = 0, 1, 2
 PRECISIONS = {"fp64": FP64, "fp64_exact": FP64_EXACT, "mixed": MIXED}
-SOLVERS = {"hlle": 0, "hlld": 1}
+SOLVERS = {"hlle": 0, "hlld": 1, "hllc": 2}
 LIMITERS = {"pcm": 0, "mc": 1, "minmod": 2, "weno5z": 3, "mp5": 4, "mp7": 5}
 BCS = {"outflow": 0, "periodic": 1}
 

@@ -49,8 +49,8 @@ int check_grid(const hlld_grid2d_t *g) {
     if (g->ng < need[g->limiter])
         return fail(HLLD_ERR_INVALID, "ng = %d is too narrow for the limiter (needs %d)", g->ng,
                     need[g->limiter]);
-    if (g->solver != HLLD_SOLVER_HLLE && g->solver != HLLD_SOLVER_HLLD)
-        return fail(HLLD_ERR_INVALID, "solver must be HLLE or HLLD");
+    if (g->solver != HLLD_SOLVER_HLLE && g->solver != HLLD_SOLVER_HLLD && g->solver != HLLD_SOLVER_HLLC)
+        return fail(HLLD_ERR_INVALID, "solver must be HLLE, HLLD or HLLC");
     if (!(g->gamma > 1.0)) return fail(HLLD_ERR_INVALID, "gamma must be > 1");
     if (!(g->dx > 0.0) || !(g->dy > 0.0)) return fail(HLLD_ERR_INVALID, "dx, dy must be > 0");
     if (!step_precision(g->precision))
@@ -155,8 +155,8 @@ int hlld_riemann_faces(int64_t n, const void *const *sL, const void *const *sR, 
                        hlld_flux_diag_t *diag, void *stream) {
     if (n < 0 || !sL || !sR || !F || !pstar) return fail(HLLD_ERR_INVALID, "bad arguments");
     if (idir < 0 || idir > 2) return fail(HLLD_ERR_INVALID, "idir must be 0, 1 or 2");
-    if (solver != HLLD_SOLVER_HLLE && solver != HLLD_SOLVER_HLLD)
-        return fail(HLLD_ERR_INVALID, "solver must be HLLE or HLLD");
+    if (solver != HLLD_SOLVER_HLLE && solver != HLLD_SOLVER_HLLD && solver != HLLD_SOLVER_HLLC)
+        return fail(HLLD_ERR_INVALID, "solver must be HLLE, HLLD or HLLC");
     if (!(gamma > 1.0)) return fail(HLLD_ERR_INVALID, "gamma must be > 1");
     if (!fp64_precision(precision)) return fail(HLLD_ERR_UNSUPPORTED, "precision %d", precision);
     cudaStream_t st = (cudaStream_t)stream;
@@ -290,7 +290,7 @@ int hlld_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
     static const int need[6] = {1, 1, 1, 2, 2, 3};
     if (b->ng < need[b->limiter]) return fail(HLLD_ERR_INVALID, "ng too narrow for the limiter");
     if (b->solver != HLLD_SOLVER_HLLE && b->solver != HLLD_SOLVER_HLLD)
-        return fail(HLLD_ERR_INVALID, "solver must be HLLE or HLLD");
+        return fail(HLLD_ERR_INVALID, "the tube kernel takes HLLE or HLLD");
     if (b->scheme != 2 && b->scheme != 3) return fail(HLLD_ERR_INVALID, "scheme must be 2 or 3");
     if (b->flavor < HLLD_TUBE_RK_STEP || b->flavor > HLLD_TUBE_DRIVER1D_CFL)
         return fail(HLLD_ERR_INVALID, "unknown tube flavor %d", b->flavor);
@@ -367,6 +367,8 @@ int hlld_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
     if (rc) return rc;
     if (g->precision != HLLD_FP64)
         return fail(HLLD_ERR_UNSUPPORTED, "the adjoint is implemented for HLLD_FP64");
+    if (g->solver == HLLD_SOLVER_HLLC)
+        return fail(HLLD_ERR_UNSUPPORTED, "the adjoint is implemented for HLLE and HLLD");
     if ((rc = check_state(s_in)) || (rc = check_state(s_out)) || (rc = check_state(lam))) return rc;
     if (scheme != 2 && scheme != 3) return fail(HLLD_ERR_INVALID, "scheme must be 2 or 3");
     if (!(dt > 0.0)) return fail(HLLD_ERR_INVALID, "dt must be > 0");

@@ -259,6 +259,8 @@ __global__ void __launch_bounds__(kThreads) riemann_faces_kernel(const FacesPara
         bool want_u = p.U[0] != nullptr;
         if (SOLVER == HLLD_SOLVER_HLLD)
             hlld_face<IDIR, double>(PL, PR, p.gamma, want_u, o);
+        else if (SOLVER == HLLD_SOLVER_HLLC)
+            hllc_face<IDIR, double>(PL, PR, p.gamma, want_u, o);
         else
             hlle_face<IDIR, double>(PL, PR, p.gamma, want_u, true, o);
 #pragma unroll
@@ -457,6 +459,8 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         FaceOut<T> o;
         if (SOLVER == HLLD_SOLVER_HLLD)
             hlld_face<AXIS, T, RB, double>(PL, PR, (T)g.gamma, false, o);
+        else if (SOLVER == HLLD_SOLVER_HLLC)
+            hllc_face<AXIS, T>(PL, PR, (T)g.gamma, false, o);
         else
             hlle_face<AXIS, T>(PL, PR, (T)g.gamma, false, false, o);
         const int64_t fi = e;
@@ -1096,6 +1100,8 @@ static void launch_faces_idir(int solver, const FacesParams &fp, cudaStream_t st
     unsigned nb = grid1d(fp.n);
     if (solver == HLLD_SOLVER_HLLD)
         riemann_faces_kernel<IDIR, HLLD_SOLVER_HLLD><<<nb, kThreads, 0, st>>>(fp);
+    else if (solver == HLLD_SOLVER_HLLC)
+        riemann_faces_kernel<IDIR, HLLD_SOLVER_HLLC><<<nb, kThreads, 0, st>>>(fp);
     else
         riemann_faces_kernel<IDIR, HLLD_SOLVER_HLLE><<<nb, kThreads, 0, st>>>(fp);
 }
@@ -1167,6 +1173,8 @@ static void launch_sweep_lim(int solver, const SweepParams &sp, cudaStream_t st)
     const int64_t nf = AXIS == 0 ? (int64_t)(sp.g.nxt + 1) * sp.g.nyt : (int64_t)sp.g.nxt * (sp.g.nyt + 1);
     if (solver == HLLD_SOLVER_HLLD)
         sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLD><<<grid1d(nf), kThreads, 0, st>>>(sp);
+    else if (solver == HLLD_SOLVER_HLLC)
+        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLC><<<grid1d(nf), kThreads, 0, st>>>(sp);
     else
         sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLE><<<grid1d(nf), kThreads, 0, st>>>(sp);
 }

@@ -658,6 +658,107 @@ __device__ __forceinline__ void hlle_face(const T *PL, const T *PR, T gamma, boo
     o.flags = 0;
 }
 
+// ── HLLC (hlld.py:1549-1765) ──────────────────────────────────────────────
+
+// hllc_flux for one face: contact speed from the HLL state (minus root of the
+// magnetised quadratic), star states on both sides, region at xi = 0, and the
+// HLL flux where the contact is degenerate / superluminal or a result is not
+// finite.  pstar gets the p_hll the reference returns in that slot.
+template <int IDIR, typename T>
+__device__ __forceinline__ void hllc_face(const T *PL, const T *PR, T gamma, bool want_u,
+                                          FaceOut<T> &o) {
+    constexpr int t1 = (IDIR + 1) % 3, t2 = (IDIR + 2) % 3;
+    constexpr int Sn = C_SX + IDIR, S1 = C_SX + t1, S2 = C_SX + t2;
+    constexpr int Bn = C_BX + IDIR, B1 = C_BX + t1, B2 = C_BX + t2;
+    Phys<T> ph;
+    srmhd_fluxes<IDIR>(PL, PR, gamma, ph);
+    const T cmin = ph.cmin, cmax = ph.cmax;
+    const T S_L = -cmin, S_R = cmax;
+    T fH[NCONS], uH[NCONS];
+#pragma unroll
+    for (int k = 0; k < NCONS; ++k) {
+        fH[k] = hf(ph.L.f[k], ph.R.f[k], ph.L.u[k], ph.R.u[k], cmin, cmax);
+        uH[k] = hu(ph.L.f[k], ph.R.f[k], ph.L.u[k], ph.R.u[k], cmin, cmax);
+    }
+    const T BG = ph.L.u[Bn];
+    const bool has_B = fabs(BG) > T(1e-15);
+    const T cross = has_B ? uH[B1] * fH[B1] + uH[B2] * fH[B2] : T(0);
+    const T bt2 = has_B ? uH[B1] * uH[B1] + uH[B2] * uH[B2] : T(0);
+    const T fbt2 = has_B ? fH[B1] * fH[B1] + fH[B2] * fH[B2] : T(0);
+    const T E_hll = uH[C_TAU] + uH[C_D];
+    const T fE_hll = fH[C_TAU] + fH[C_D];
+    const T qa = fE_hll - cross;
+    const T qb = -fH[Sn] - E_hll + bt2 + fbt2;
+    const T qc = uH[Sn] - cross;
+    const T disc = sqrt(clamp_lo(qb * qb - T(4) * qa * qc, T(0)));
+    const T vc_quad = sdiv(T(-0.5) * (qb + disc), qa);
+    const T vc_lin = sdiv(-qc, qb);
+    const T vc = fabs(qa) < T(1e-15) ? (fabs(qb) < T(1e-15) ? T(0) : vc_lin) : vc_quad;
+    const T vt1 = has_B ? sdiv(uH[B1] * vc - fH[B1], BG) : T(0);
+    const T vt2 = has_B ? sdiv(uH[B2] * vc - fH[B2], BG) : T(0);
+    const T v2 = vc * vc + vt1 * vt1 + vt2 * vt2;
+    const T v2s = clamp_hi(v2, T(1) - T(1e-10));
+    const T gs = T(1) / sqrt(T(1) - v2s);
+    const T vsBs = has_B ? vc * uH[Bn] + vt1 * uH[B1] + vt2 * uH[B2] : T(0);
+    const T bgs = BG / gs;
+    const T p_star = has_B ? fH[Sn] + bgs * bgs - vc * (fH[C_TAU] + fH[C_D] - BG * vsBs)
+                           : fH[Sn] - vc * (fH[C_TAU] + fH[C_D]);
+    const bool degen = (vc <= S_L) || (vc >= S_R) || (v2 >= T(1));
+    // region at xi = 0, in the reference's order of overrides: L, *L, *R, R
+    // (-1: none applies, the HLL state stays)
+    int reg = -1;
+    if (T(0) <= S_L) reg = 0;
+    if (S_L < T(0) && T(0) < vc) reg = 1;
+    if (vc <= T(0) && T(0) < S_R) reg = 2;
+    if (T(0) >= S_R) reg = 3;
+    T uc[NCONS];
+    if (!degen && (reg == 1 || reg == 2)) {
+        const Side<T> &sd = reg == 1 ? ph.L : ph.R;
+        const T SK = reg == 1 ? S_L : S_R;
+        const T vdK = (reg == 1 ? PL : PR)[P_VX + IDIR];
+        const T denom = SK - vc;
+        uc[Bn] = BG;
+        uc[B1] = uH[B1];
+        uc[B2] = uH[B2];
+        uc[C_D] = sdiv(sd.u[C_D] * (SK - vdK), denom);
+        uc[C_TAU] = sdiv(SK * sd.u[C_TAU] - sd.f[C_TAU] + p_star * vc - vsBs * BG, denom);
+        uc[Sn] = (uc[C_TAU] + uc[C_D] + p_star) * vc - vsBs * BG;
+        const T gs2 = gs * gs;
+        uc[S1] = has_B ? sdiv(-BG * (uH[B1] / gs2 + vsBs * vt1) - sd.f[S1] + SK * sd.u[S1], denom)
+                       : sdiv(sd.u[S1] * (SK - vdK), denom);
+        uc[S2] = has_B ? sdiv(-BG * (uH[B2] / gs2 + vsBs * vt2) - sd.f[S2] + SK * sd.u[S2], denom)
+                       : sdiv(sd.u[S2] * (SK - vdK), denom);
+    }
+#pragma unroll
+    for (int k = 0; k < NCONS; ++k) {
+        T f = fH[k], u = uH[k];
+        if (!degen && reg >= 0) {
+            if (reg == 0) {
+                f = ph.L.f[k];
+                u = ph.L.u[k];
+            } else if (reg == 3) {
+                f = ph.R.f[k];
+                u = ph.R.u[k];
+            } else {
+                const Side<T> &sd = reg == 1 ? ph.L : ph.R;
+                const T SK = reg == 1 ? S_L : S_R;
+                f = sd.f[k] + SK * (uc[k] - sd.u[k]);
+                u = uc[k];
+            }
+        }
+        if (!isfinite(real_of(f)) || !isfinite(real_of(u))) {
+            f = fH[k];
+            u = uH[k];
+        }
+        o.F[k] = f;
+        if (want_u) o.U[k] = u;
+    }
+    o.pstar = hlle_p_estimate(PL, PR, gamma);
+    o.err = 0;
+    o.iters = 0;
+    o.flags = 0;
+}
+
 // ── HLLD (hlld.py:366-605, :669-746, :1202-1543) ─────────────────────────
 
 // HLLDComputation R vectors (hlld.py:401-428), energy form

@@ -6,8 +6,8 @@ eight conserved components, p_star < 0 marks an HLLE-fallback face
 (``hlld.py:1531``).  The arithmetic runs in the CUDA kernels of
 libhlld_b200.so (``hlld_riemann_faces``); inputs must be float64 CUDA
 tensors.  ``hlld_flux`` refreshes the module-global ``LAST_DIAG`` as the
-reference does (``hlld.py:1098``, ``:1516-1529``); ``hlle_flux`` leaves it
-alone, as the reference's does.
+reference does (``hlld.py:1098``, ``:1516-1529``); ``hlle_flux`` and
+``hllc_flux`` leave it alone, as the reference's do.
 """
 from __future__ import annotations
 
@@ -92,6 +92,12 @@ def hlle_flux(sL, sR, eos, idir: int = 0, precision: str = "fp64"):
     return F, U, ps
 
 
+def hllc_flux(sL, sR, eos, idir: int = 0, precision: str = "fp64"):
+    """hlld.py:1549-1765; the third output is p_hll, as in the reference."""
+    F, U, ps, *_ = riemann(sL, sR, eos, idir, "hllc", precision)
+    return F, U, ps
+
+
 def primitive_to_conserved(prim: dict, precision: str = "fp64") -> dict:
     """hlld.py:185-217"""
     tensors = [_lib.require_cuda(prim[k], f"prim[{k!r}]") for k in PRIM_KEYS]
@@ -106,7 +112,7 @@ def primitive_to_conserved(prim: dict, precision: str = "fp64") -> dict:
     return {k: c.reshape(shape) for k, c in zip(CONS_KEYS, C)}
 
 
-SOLVERS = {"hlld": hlld_flux, "hlle": hlle_flux}
+SOLVERS = {"hlld": hlld_flux, "hlle": hlle_flux, "hllc": hllc_flux}
 
 
 def solver_name(flux_fn) -> str:
@@ -115,7 +121,8 @@ def solver_name(flux_fn) -> str:
         name = flux_fn
     else:
         name = getattr(flux_fn, "__name__", "")
-        name = {"hlld_flux": "hlld", "hlle_flux": "hlle"}.get(name, name)
-    if name not in ("hlld", "hlle"):
-        raise NotImplementedError(f"flux_fn {name!r}: the B200 step implements hlld and hlle")
+        name = {"hlld_flux": "hlld", "hlle_flux": "hlle", "hllc_flux": "hllc"}.get(name, name)
+    if name not in ("hlld", "hlle", "hllc"):
+        raise NotImplementedError(f"flux_fn {name!r}: the B200 step implements hlld, hlle "
+                                  "and hllc")
     return name

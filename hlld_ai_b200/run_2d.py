@@ -27,7 +27,7 @@ from .physics.initial_data2d import PROBLEMS, orszag_tang, setup_problem
 from .physics.reconstruction import ghosts_needed
 from .physics.state import EVOLVED_KEYS, State2D
 
-SOLVERS = ("hlld", "hlle")
+SOLVERS = ("hlld", "hlle", "hllc")
 
 
 def _bs(grid, eos):

@@ -42,7 +42,9 @@ enum hlld_precision {
     HLLD_FP64_EXACT = 1, /* FP64, one rounding per operation (reference order) */
     HLLD_MIXED = 2       /* FP32 reconstruction/fluxes/update, FP64 C2P, p*, RK state */
 };
-enum hlld_solver { HLLD_SOLVER_HLLE = 0, HLLD_SOLVER_HLLD = 1 };
+/* HLLE: hlld.py:1005-1044; HLLD: :1202-1543; HLLC: :1549-1765 (flux plugin
+ * and 2D step; the tube kernel and the adjoint take HLLE and HLLD) */
+enum hlld_solver { HLLD_SOLVER_HLLE = 0, HLLD_SOLVER_HLLD = 1, HLLD_SOLVER_HLLC = 2 };
 enum hlld_limiter {
     HLLD_LIM_PCM = 0, HLLD_LIM_MC = 1, HLLD_LIM_MINMOD = 2,
     HLLD_LIM_WENO5Z = 3, HLLD_LIM_MP5 = 4, HLLD_LIM_MP7 = 5

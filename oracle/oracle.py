@@ -21,7 +21,7 @@ PRIM_KEYS = ("rho", "vx", "vy", "vz", "p", "eps", "Bx", "By", "Bz")
 CONS_KEYS = ("D", "Sx", "Sy", "Sz", "tau", "Bx", "By", "Bz")
 EVOLVED_KEYS = ("D", "Sx", "Sy", "Sz", "tau", "Bz")
 LIMITERS = {"pcm": 0, "mc": 1, "minmod": 2, "weno5z": 3, "mp5": 4, "mp7": 5}
-SOLVERS = {"hlle": 0, "hlld": 1}
+SOLVERS = {"hlle": 0, "hlld": 1, "hllc": 2}
 BCS = {"outflow": 0, "periodic": 1}
 
 ST_BRACKET_OK, ST_CONVERGED, ST_V_CLAMPED, ST_ATMO, ST_BISECTED = 1, 2, 4, 8, 16

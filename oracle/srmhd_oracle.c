@@ -822,11 +822,97 @@ static void hlld_one(const double *PL, const double *PR, int idir, double gamma,
                                (bn_zero ? ORC_RF_BN_ZERO : 0) | (failed ? ORC_RF_FAILED : 0));
 }
 
+/* hlld.py:1549-1765 hllc_flux for one face; pstar gets the p_hll the
+ * reference returns in that slot */
+static void hllc_one(const double *PL, const double *PR, int idir, double gamma, double *F,
+                     double *U, double *pstar) {
+    phys_t ph;
+    compute_srmhd_fluxes(PL, PR, idir, gamma, &ph);
+    const int t1 = (idir + 1) % 3, t2 = (idir + 2) % 3;
+    const int Sn = ORC_SX + idir, S1 = ORC_SX + t1, S2 = ORC_SX + t2;
+    const int Bn = ORC_BX + idir, B1 = ORC_BX + t1, B2 = ORC_BX + t2;
+    const double cmin = ph.cmin, cmax = ph.cmax;
+    const double S_L = -cmin, S_R = cmax;
+    double fH[ORC_NCONS], uH[ORC_NCONS];
+    for (int k = 0; k < ORC_NCONS; ++k) {
+        fH[k] = hf(ph.L.f[k], ph.R.f[k], ph.L.u[k], ph.R.u[k], cmin, cmax);
+        uH[k] = hu(ph.L.f[k], ph.R.f[k], ph.L.u[k], ph.R.u[k], cmin, cmax);
+    }
+    const double BG = ph.L.u[Bn];
+    const int has_B = fabs(BG) > 1e-15;
+    /* contact speed (quadratic, minus root) */
+    const double cross = has_B ? uH[B1] * fH[B1] + uH[B2] * fH[B2] : 0.0;
+    const double bt2 = has_B ? uH[B1] * uH[B1] + uH[B2] * uH[B2] : 0.0;
+    const double fbt2 = has_B ? fH[B1] * fH[B1] + fH[B2] * fH[B2] : 0.0;
+    const double E_hll = uH[ORC_TAU] + uH[ORC_D];
+    const double fE_hll = fH[ORC_TAU] + fH[ORC_D];
+    const double qa = fE_hll - cross;
+    const double qb = -fH[Sn] - E_hll + bt2 + fbt2;
+    const double qc = uH[Sn] - cross;
+    const double disc = sqrt(clamp_lo(qb * qb - 4.0 * qa * qc, 0.0));
+    const double vc_quad = sdiv(-0.5 * (qb + disc), qa);
+    const double vc_lin = sdiv(-qc, qb);
+    const double vc = fabs(qa) < 1e-15 ? (fabs(qb) < 1e-15 ? 0.0 : vc_lin) : vc_quad;
+    /* star-region transverse velocities, Lorentz factor, v*.B* */
+    const double vt1 = has_B ? sdiv(uH[B1] * vc - fH[B1], BG) : 0.0;
+    const double vt2 = has_B ? sdiv(uH[B2] * vc - fH[B2], BG) : 0.0;
+    const double v2 = vc * vc + vt1 * vt1 + vt2 * vt2;
+    const double v2s = clamp_hi(v2, 1.0 - 1e-10);
+    const double gs = 1.0 / sqrt(1.0 - v2s);
+    const double vsBs = has_B ? vc * uH[Bn] + vt1 * uH[B1] + vt2 * uH[B2] : 0.0;
+    const double bgs = BG / gs;
+    const double p_star = has_B ? fH[Sn] + bgs * bgs - vc * (fH[ORC_TAU] + fH[ORC_D] - BG * vsBs)
+                                : fH[Sn] - vc * (fH[ORC_TAU] + fH[ORC_D]);
+    /* star states */
+    double uc[2][ORC_NCONS], fs[2][ORC_NCONS];
+    for (int side = 0; side < 2; ++side) {
+        const side_t *sd = side == 0 ? &ph.L : &ph.R;
+        const double SK = side == 0 ? S_L : S_R;
+        const double vdK = (side == 0 ? PL : PR)[ORC_VX + idir];
+        const double denom = SK - vc;
+        double *c = uc[side];
+        c[Bn] = BG;
+        c[B1] = uH[B1];
+        c[B2] = uH[B2];
+        c[ORC_D] = sdiv(sd->u[ORC_D] * (SK - vdK), denom);
+        c[ORC_TAU] = sdiv(SK * sd->u[ORC_TAU] - sd->f[ORC_TAU] + p_star * vc - vsBs * BG, denom);
+        c[Sn] = (c[ORC_TAU] + c[ORC_D] + p_star) * vc - vsBs * BG;
+        const double gs2 = gs * gs;
+        const double St1B = sdiv(-BG * (uH[B1] / gs2 + vsBs * vt1) - sd->f[S1] + SK * sd->u[S1], denom);
+        const double St2B = sdiv(-BG * (uH[B2] / gs2 + vsBs * vt2) - sd->f[S2] + SK * sd->u[S2], denom);
+        const double St10 = sdiv(sd->u[S1] * (SK - vdK), denom);
+        const double St20 = sdiv(sd->u[S2] * (SK - vdK), denom);
+        c[S1] = has_B ? St1B : St10;
+        c[S2] = has_B ? St2B : St20;
+        for (int k = 0; k < ORC_NCONS; ++k) fs[side][k] = sd->f[k] + SK * (c[k] - sd->u[k]);
+    }
+    /* region at xi = 0, then the degenerate / superluminal and non-finite
+     * fallbacks to the HLL state */
+    const int degen = (vc <= S_L) || (vc >= S_R) || (v2 >= 1.0);
+    for (int k = 0; k < ORC_NCONS; ++k) {
+        double f = fH[k], u = uH[k];
+        if (0.0 <= S_L) { f = ph.L.f[k]; u = ph.L.u[k]; }
+        if (S_L < 0.0 && 0.0 < vc) { f = fs[0][k]; u = uc[0][k]; }
+        if (vc <= 0.0 && 0.0 < S_R) { f = fs[1][k]; u = uc[1][k]; }
+        if (0.0 >= S_R) { f = ph.R.f[k]; u = ph.R.u[k]; }
+        if (degen) { f = fH[k]; u = uH[k]; }
+        if (!isfinite(f) || !isfinite(u)) { f = fH[k]; u = uH[k]; }
+        F[k] = f;
+        U[k] = u;
+    }
+    *pstar = hlle_p_estimate(PL, PR, gamma);
+}
+
 static void riemann_one(const double *PL, const double *PR, int idir, int solver, double gamma,
                         double *F, double *U, double *pstar, int32_t *err, int32_t *iters,
                         uint8_t *flags) {
     if (solver == ORC_SOLVER_HLLD) {
         hlld_one(PL, PR, idir, gamma, F, U, pstar, err, iters, flags);
+    } else if (solver == ORC_SOLVER_HLLC) {
+        hllc_one(PL, PR, idir, gamma, F, U, pstar);
+        if (err) *err = 0;
+        if (iters) *iters = 0;
+        if (flags) *flags = 0;
     } else {
         hlle_one(PL, PR, idir, gamma, F, U, pstar);
         if (err) *err = 0;

@@ -54,7 +54,7 @@ enum { ORC_D = 0, ORC_SX, ORC_SY, ORC_SZ, ORC_TAU, ORC_BX, ORC_BY, ORC_BZ, ORC_N
 #define ORC_RF_BN_ZERO 2u
 #define ORC_RF_FAILED 4u
 
-enum { ORC_SOLVER_HLLE = 0, ORC_SOLVER_HLLD = 1 };
+enum { ORC_SOLVER_HLLE = 0, ORC_SOLVER_HLLD = 1, ORC_SOLVER_HLLC = 2 };
 enum { ORC_LIM_PCM = 0, ORC_LIM_MC = 1, ORC_LIM_MINMOD = 2, ORC_LIM_WENO5Z = 3, ORC_LIM_MP5 = 4, ORC_LIM_MP7 = 5 };
 enum { ORC_BC_OUTFLOW = 0, ORC_BC_PERIODIC = 1 };
 

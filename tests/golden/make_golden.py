@@ -18,6 +18,9 @@ inputs, the outputs the oracle is pinned against (tests/test_oracle_golden.py):
   tube1d.npz   six rk2_step steps of the 800-cell Brio-Wu tube (PLM-MC, HLLD)
   tubes.npz    three batched-workload tubes (WENO5-Z, HLLD, SSP-RK3): driver2d
                rk_step on ny = 1 grids with driver.compute_dt, four steps each
+  hllc.npz     hllc_flux for idir 0-2 on 512 seeded face pairs, a quarter of
+               them with zero normal field (``python make_golden.py REF hllc``
+               writes only this file)
 
 The reference is not needed to run the tests; only this script reads it.
 """
@@ -291,5 +294,62 @@ def main(ref_root: str) -> None:
     print("golden vectors written to", HERE)
 
 
+def make_hllc(ref_root: str) -> None:
+    """hllc.npz: the reference's hllc_flux (hlld.py:1549-1765)."""
+    sys.dont_write_bytecode = True
+    sys.path.insert(0, ref_root)
+    import torch
+    from src.physics.eos import hybrid_eos
+    from src.physics.hlld import hllc_flux
+
+    PK = ("rho", "vx", "vy", "vz", "p", "eps", "Bx", "By", "Bz")
+    CK = ("D", "Sx", "Sy", "Sz", "tau", "Bx", "By", "Bz")
+    G = 5.0 / 3.0
+    eos = hybrid_eos(K=0.0, gamma=G, gamma_th=G)
+    n = 512
+    g = torch.Generator().manual_seed(20261203)
+
+    def u(lo, hi):
+        return torch.empty(n, dtype=torch.float64).uniform_(lo, hi, generator=g)
+
+    def one():
+        rho = 10.0 ** u(-1.0, 1.0)
+        p = 10.0 ** u(-1.5, 1.0)
+        W = 1.0 + 10.0 ** u(-3.0, math.log10(4.0))
+        sp = torch.sqrt(1.0 - 1.0 / W**2)
+        th, ph = u(0, math.pi), u(0, 2 * math.pi)
+        s = {"rho": rho, "p": p, "vx": sp * torch.sin(th) * torch.cos(ph),
+             "vy": sp * torch.sin(th) * torch.sin(ph), "vz": sp * torch.cos(th),
+             "Bx": u(-3, 3), "By": u(-3, 3), "Bz": u(-3, 3)}
+        s["eps"] = eos.eps__press_rho(s["p"], s["rho"])
+        return s
+
+    sL, sR = one(), one()
+    for k in ("Bx", "By", "Bz"):
+        sR[k] = sL[k].clone()
+    out = {"gamma": np.float64(G)}
+    for idir in (0, 1, 2):
+        bk = ("Bx", "By", "Bz")[idir]
+        L = {k: v.clone() for k, v in sL.items()}
+        R = {k: v.clone() for k, v in sR.items()}
+        L[bk][: n // 4] = 0.0
+        R[bk][: n // 4] = 0.0
+        for k in PK:
+            out[f"{idir}_L_{k}"] = L[k].numpy()
+            out[f"{idir}_R_{k}"] = R[k].numpy()
+        F, U, ps = hllc_flux(L, R, eos, idir=idir)
+        for k in CK:
+            out[f"{idir}_F_{k}"] = F[k].numpy()
+            out[f"{idir}_U_{k}"] = U[k].numpy()
+        out[f"{idir}_pstar"] = ps.numpy()
+    np.savez_compressed(os.path.join(HERE, "hllc.npz"), **out)
+    print("hllc.npz written to", HERE)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) > 2 and sys.argv[2] == "hllc":
+        make_hllc(root)
+    else:
+        main(root)
+        make_hllc(root)

@@ -109,7 +109,7 @@ def test_prim_to_cons_vjp_matches_central_difference():
     lp = prim_to_cons_vjp(prims, lam)
     from hlld_ai_b200.physics.driver2d import prims_to_cons_2d
     for k in ("rho", "vx", "p", "eps", "By"):
-        h = 1e-7 * (float(prims[k].abs().max()) + 1e-3)
+        h = 1e-7 * (float(prims[k].abs().max()) + 1.0)
         pp = dict(prims)
         pm = dict(prims)
         pp[k] = prims[k] + h

@@ -1,4 +1,4 @@
-"""Per-face HLLE/HLLD kernels (the flux_fn plugin) against the CPU oracle.
+"""Per-face HLLE/HLLD/HLLC kernels (the flux_fn plugin) against the CPU oracle.
 
 FP64-exact build: bitwise equal to the oracle.  FP64 (FMA) build: the
 tolerances of the reference's direction-genericity test
@@ -29,7 +29,7 @@ def states():
     return to_np(sL), to_np(sR)
 
 
-@pytest.mark.parametrize("solver", ["hlle", "hlld"])
+@pytest.mark.parametrize("solver", ["hlle", "hlld", "hllc"])
 @pytest.mark.parametrize("idir", [0, 1, 2])
 def test_exact_build_is_bitwise_oracle(states, solver, idir):
     nL, nR = states
@@ -102,3 +102,19 @@ def test_cpu_tensors_are_rejected(states):
     cpu = {k: torch.as_tensor(v) for k, v in nL.items()}
     with pytest.raises(TypeError):
         H.hlld_flux(cpu, cpu, EOS)
+
+
+@pytest.mark.parametrize("idir", [0, 1, 2])
+def test_hllc_matches_reference_golden(idir):
+    """hllc_flux against the reference's own output (tests/golden/hllc.npz,
+    a quarter of the faces with zero normal field): FP64-exact build."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "hllc.npz"))
+    keys = ["rho", "vx", "vy", "vz", "p", "eps", "Bx", "By", "Bz"]
+    L = {k: torch.tensor(z[f"{idir}_L_{k}"], device="cuda") for k in keys}
+    R = {k: torch.tensor(z[f"{idir}_R_{k}"], device="cuda") for k in keys}
+    F, U, ps = Hh.hllc_flux(L, R, EOS, idir=idir, precision="fp64_exact")
+    for k in ("D", "Sx", "Sy", "Sz", "tau", "Bx", "By", "Bz"):
+        assert max_rel(z[f"{idir}_F_{k}"], F[k].cpu().numpy()) < 1e-12, k
+        assert max_rel(z[f"{idir}_U_{k}"], U[k].cpu().numpy()) < 1e-12, k
+    assert max_rel(z[f"{idir}_pstar"], ps.cpu().numpy()) < 1e-14

@@ -85,6 +85,8 @@ CASES = [
     ("rotor", 24, 24, "minmod", "hlld"),
     ("orszag_tang", 24, 24, "pcm", "hlld"),
     ("orszag_tang", 24, 24, "mp7", "hlld"),
+    ("rotor", 32, 32, "mc", "hllc"),
+    ("orszag_tang", 28, 28, "weno5z", "hllc"),
 ]
 
 

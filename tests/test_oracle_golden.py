@@ -236,3 +236,17 @@ def test_tube_run_resumes_from_its_conserved_state():
                        resume=True, max_steps=2)
     for k in PK:
         assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("idir", [0, 1, 2])
+def test_hllc_matches_reference(idir):
+    """hlld.py:1549-1765 hllc_flux on 512 seeded faces (a quarter with zero
+    normal field): fluxes, states and the p_hll slot."""
+    z = load("hllc.npz")
+    L = {k: z[f"{idir}_L_{k}"] for k in PK}
+    R = {k: z[f"{idir}_R_{k}"] for k in PK}
+    F, U, ps = oracle.riemann(L, R, idir, "hllc", float(z["gamma"]))[:3]
+    for k in CK:
+        assert max_rel(z[f"{idir}_F_{k}"], F[k]) < 1e-12, k
+        assert max_rel(z[f"{idir}_U_{k}"], U[k]) < 1e-12, k
+    assert max_rel(z[f"{idir}_pstar"], ps) < 1e-14
