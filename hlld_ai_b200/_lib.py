@@ -100,6 +100,17 @@ SIGNATURES = {
     "hlld_prim_to_cons_vjp": (ctypes.c_int, [ctypes.c_int64, _PP, _PP, _PP, _VP]),
     "hlld_adjoint_scratch_bytes": (ctypes.c_int, [ctypes.POINTER(Grid2DC),
                                                   ctypes.POINTER(ctypes.c_size_t)]),
+    "hlld_adjoint_tape_bytes": (ctypes.c_int, [ctypes.POINTER(Grid2DC),
+                                               ctypes.POINTER(ctypes.c_size_t),
+                                               ctypes.POINTER(ctypes.c_size_t)]),
+    "hlld_adjoint_record_step": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
+                                                ctypes.c_double, ctypes.c_int, _VP, ctypes.c_size_t,
+                                                _VP, ctypes.c_size_t, _VP]),
+    "hlld_adjoint_reverse_step": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
+                                                 ctypes.POINTER(State2DC), ctypes.c_double,
+                                                 ctypes.c_int, _VP, ctypes.c_size_t,
+                                                 ctypes.POINTER(State2DC), _VP, ctypes.c_size_t,
+                                                 _VP]),
     "hlld_adjoint_rk_step_ct": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
                                                ctypes.POINTER(State2DC), ctypes.c_double,
                                                ctypes.c_int, ctypes.POINTER(State2DC), _VP,

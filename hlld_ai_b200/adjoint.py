@@ -2,9 +2,10 @@
 
 ``CheckpointedRun`` runs the FP64 2D step forward for a fixed sequence of
 time steps, keeping the state every ``checkpoint_every`` steps, and runs the
-adjoint backward: each segment is recomputed from its checkpoint (all its
-step states kept), then the steps are reversed one by one with
-``hlld_adjoint_rk_step_ct``, the transpose of the step's Jacobian with the
+adjoint backward: each segment is recomputed once from its checkpoint with
+``hlld_adjoint_record_step`` (the step states and each step's tape kept),
+then the steps are reversed one by one with ``hlld_adjoint_reverse_step``,
+the transpose of the step's Jacobian with the
 time step fixed and every discrete decision frozen at its forward outcome
 (limiter branches, HLLD region and fallback, CT upwind signs); the HLLD p*
 and the Kastaun C2P root are differentiated by the implicit-function
@@ -63,6 +64,13 @@ class CheckpointedRun:
         self._scratch = torch.empty(n.value + 256, dtype=torch.uint8, device=self.device)
         self._scratch_ptr = (self._scratch.data_ptr() + 255) // 256 * 256
         self._scratch_bytes = n.value
+        tb, rb = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        _lib.check(_lib.lib().hlld_adjoint_tape_bytes(ctypes.byref(self.stepper.gc),
+                                                      ctypes.byref(tb), ctypes.byref(rb)),
+                   "hlld_adjoint_tape_bytes")
+        self._tape_bytes = tb.value
+        assert rb.value <= self._scratch_bytes
+        self._tapes: list[torch.Tensor] = []
         self.checkpoints: list[State2D] = []
         self.dts: list[float] = []
 
@@ -91,6 +99,34 @@ class CheckpointedRun:
                 _lib.stream_handle(self.device))
         _lib.check(rc, "hlld_adjoint_rk_step_ct")
 
+    def _tape(self, k: int) -> int:
+        while len(self._tapes) <= k:
+            self._tapes.append(torch.empty(self._tape_bytes + 256, dtype=torch.uint8,
+                                           device=self.device))
+        return (self._tapes[k].data_ptr() + 255) // 256 * 256
+
+    def record_step(self, s: State2D, dt: float, k: int) -> None:
+        """One forward step of s in place, recording tape k."""
+        st = self.stepper
+        a = st._struct(s)
+        with torch.cuda.device(self.device):
+            rc = _lib.lib().hlld_adjoint_record_step(
+                ctypes.byref(st.gc), ctypes.byref(a), float(dt), _SCHEMES[self.scheme],
+                self._tape(k), self._tape_bytes, self._scratch_ptr, self._scratch_bytes,
+                _lib.stream_handle(self.device))
+        _lib.check(rc, "hlld_adjoint_record_step")
+
+    def reverse_step(self, s_in: State2D, s_out: State2D, dt: float, k: int, lam: State2D) -> None:
+        """lam: gradient w.r.t. s_out -> w.r.t. s_in (in place), from tape k."""
+        st = self.stepper
+        a, b, l = st._struct(s_in), st._struct(s_out), st._struct(lam)
+        with torch.cuda.device(self.device):
+            rc = _lib.lib().hlld_adjoint_reverse_step(
+                ctypes.byref(st.gc), ctypes.byref(a), ctypes.byref(b), float(dt),
+                _SCHEMES[self.scheme], self._tape(k), self._tape_bytes, ctypes.byref(l),
+                self._scratch_ptr, self._scratch_bytes, _lib.stream_handle(self.device))
+        _lib.check(rc, "hlld_adjoint_reverse_step")
+
     # -- backward ---------------------------------------------------------
     def backward(self, lam: State2D) -> State2D:
         """lam: gradient of the objective with respect to the final state
@@ -107,10 +143,10 @@ class CheckpointedRun:
             states = [self.checkpoints[seg].clone()]
             for i in range(i0, i1):
                 s = states[-1].clone()
-                self.stepper.step(s, self.dts[i], self.scheme)
+                self.record_step(s, self.dts[i], i - i0)
                 states.append(s)
             for i in range(i1 - 1, i0 - 1, -1):
-                self.step_adjoint(states[i - i0], states[i - i0 + 1], self.dts[i], lam)
+                self.reverse_step(states[i - i0], states[i - i0 + 1], self.dts[i], i - i0, lam)
             del states
         return lam
 

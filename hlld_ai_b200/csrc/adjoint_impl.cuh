@@ -21,17 +21,18 @@
 //   e. RK combine and flux divergence / CT curl -> lambda of the fluxes and
 //      corner EMFs, and of U0 / U_s
 //   f. corner EMF (ct.py:119-177) -> transverse-B fluxes, cell E -> v, B
-//   g. the two sweeps: per face a Dual<15> evaluation of the Riemann solver
-//      at the forward p* (7 primitives per side + the normal field), then the
-//      primitive conversion and the reconstruction (Dual over the stencil)
-//      in reverse, gathered onto cells without atomics.
+//   g. the two sweeps: per face the Riemann solver in reverse mode at the
+//      forward p* (face_vjp.cuh), then the primitive conversion and the
+//      reconstruction (Dual over the stencil) in reverse, gathered onto
+//      cells without atomics.
 #pragma once
+
+#include "face_vjp.cuh"
 
 namespace hlld {
 namespace HLLD_NS {
 
 constexpr int kAdjDirs = 15;  // rho, p, vx, vy, vz, B_t, Bz per side + B_n
-using DR = Dual<kAdjDirs>;
 constexpr int kMaxNW = 8;     // widest reconstruction window (MP7)
 
 struct AdjSweepParams {
@@ -39,6 +40,8 @@ struct AdjSweepParams {
     const double *rho, *p, *vx, *vy, *vz, *bz;
     const double *Bxf, *Byf;
     const double *lamF[NFLUX];
+    const double *pstar_in;    // the forward sweep's p* and fallback per face
+    const uint8_t *fail_in;
     double *lamS[kMaxNW * 7];  // [slot * 7 + var] per face
     double *lamBn;
 };
@@ -138,46 +141,42 @@ __global__ void __launch_bounds__(kThreads) adj_sweep_kernel(const AdjSweepParam
     }
     double given[2] = {0.0, 0.0};
     if (SOLVER == HLLD_SOLVER_HLLD) {
-        FaceOut<double> o;
-        hlld_face<AXIS, double, double, double>(PL, PR, g.gamma, false, o);
-        given[0] = o.pstar;
-        given[1] = (o.flags & RF_FAILED) ? 1.0 : 0.0;
+        given[0] = p.pstar_in[e];
+        given[1] = p.fail_in[e] ? 1.0 : 0.0;
     }
-    // tangent of the Riemann solver in the 15 face-state directions
+    // the Riemann solver in reverse (face_vjp.cuh): flux adjoint -> the nine
+    // primitives of each face state, then eps = eps(p, rho) and the shared
+    // normal field
     double lam[kAdjDirs];
     {
-        DR DL[NPRIM], DRt[NPRIM];
+        double lF[NCONS] = {0, 0, 0, 0, 0, 0, 0, 0};
+        lF[C_D] = p.lamF[F_D][e];
+        lF[C_SX] = p.lamF[F_SX][e];
+        lF[C_SY] = p.lamF[F_SY][e];
+        lF[C_SZ] = p.lamF[F_SZ][e];
+        lF[C_TAU] = p.lamF[F_TAU][e];
+        lF[C_BZ] = p.lamF[F_BZ][e];
+        lF[AXIS == 0 ? C_BY : C_BX] = p.lamF[F_BT][e];
+        double aL[NPRIM] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, aR[NPRIM] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (SOLVER == HLLD_SOLVER_HLLD)
+            vjp::hlld_face_vjp<AXIS>(PL, PR, g.gamma, given[0], given[1] != 0.0, lF, aL, aR);
+        else
+            vjp::hlle_face_vjp<AXIS>(PL, PR, g.gamma, lF, aL, aR);
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
             const double *P = side == 0 ? PL : PR;
-            DR *Q = side == 0 ? DL : DRt;
-            const int o7 = side * 7;
-            Q[P_RHO] = DR::var(P[P_RHO], o7 + 0);
-            Q[P_P] = DR::var(P[P_P], o7 + 1);
-            Q[P_VX] = DR::var(P[P_VX], o7 + 2);
-            Q[P_VY] = DR::var(P[P_VY], o7 + 3);
-            Q[P_VZ] = DR::var(P[P_VZ], o7 + 4);
-            Q[IBT] = DR::var(P[IBT], o7 + 5);
-            Q[P_BZ] = DR::var(P[P_BZ], o7 + 6);
-            Q[IBN] = DR::var(bn, 14);
-            Q[P_EPS] = eos_eps(Q[P_P], Q[P_RHO], DR(g.gamma));
+            const double *A = side == 0 ? aL : aR;
+            double *l = lam + side * 7;
+            // eps = p / (rho (gamma - 1))
+            l[0] = A[P_RHO] - A[P_EPS] * P[P_EPS] / P[P_RHO];
+            l[1] = A[P_P] + A[P_EPS] / (P[P_RHO] * (g.gamma - 1.0));
+            l[2] = A[P_VX];
+            l[3] = A[P_VY];
+            l[4] = A[P_VZ];
+            l[5] = A[IBT];
+            l[6] = A[P_BZ];
         }
-        FaceOut<DR> od;
-        if (SOLVER == HLLD_SOLVER_HLLD)
-            hlld_face<AXIS, DR, DR, DR, true>(DL, DRt, DR(g.gamma), false, od, given);
-        else
-            hlle_face<AXIS, DR>(DL, DRt, DR(g.gamma), false, false, od);
-        const int comp[NFLUX] = {C_D, C_SX, C_SY, C_SZ, C_TAU, C_BZ, AXIS == 0 ? C_BY : C_BX};
-        double lf[NFLUX];
-#pragma unroll
-        for (int m = 0; m < NFLUX; ++m) lf[m] = p.lamF[m][e];
-#pragma unroll
-        for (int j = 0; j < kAdjDirs; ++j) {
-            double s = 0.0;
-#pragma unroll
-            for (int m = 0; m < NFLUX; ++m) s += lf[m] * od.F[comp[m]].d[j];
-            lam[j] = s;
-        }
+        lam[14] = aL[IBN] + aR[IBN];
     }
     p.lamBn[e] = lam[14];
     // reverse of the conversion W v -> v and the floors, per side
@@ -294,6 +293,7 @@ struct AdjC2PParams {
     double *lP[9];     // lambda of the primitives (read, then zeroed)
     double *lU[6];     // accumulated
     double *lBcx, *lBcy;  // accumulated
+    const double *mu_in;  // the forward's C2P roots, or NULL (solved here)
 };
 
 __global__ void __launch_bounds__(kThreads) adj_c2p_kernel(const AdjC2PParams p) {
@@ -316,7 +316,8 @@ __global__ void __launch_bounds__(kThreads) adj_c2p_kernel(const AdjC2PParams p)
     double Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
     double C[NCONS] = {p.U[0][c], p.U[1][c], p.U[2][c], p.U[3][c], p.U[4][c], Bcx, Bcy, p.U[5][c]};
     double P[NPRIM], mu = 0.0;
-    cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P, &mu);
+    if (p.mu_in) mu = p.mu_in[c];
+    else cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P, &mu);
     using D8 = Dual<NCONS>;
     D8 Cd[NCONS], Pd[NPRIM];
 #pragma unroll
@@ -680,11 +681,22 @@ struct AdjState {   // one saved stage state
     double *U[6], *Bxf, *Byf, *P[9];
 };
 
+// What the forward step records for its reverse: the inputs of stages 1
+// and 2, and per stage the F_D of both sweeps (CT upwind signs), the sweep
+// counters (their max |F_D| sets the deadband) and each face's p* and
+// HLLE fallback.
+struct AdjTape {
+    AdjState X[2];
+    double *FxD[3], *FyD[3];
+    double *psx[3], *psy[3];
+    uint8_t *fx[3], *fy[3];
+    double *mu[3];           // C2P roots of each stage's sync (the inputs of the next stage)
+    hlld_step_diag_t *diag;  // [3]
+};
+
+// Work arrays of the reverse (and of the recording forward step).
 struct AdjScratch {
-    AdjState X[2];            // stage inputs 1 and 2
-    double *FxD[3], *FyD[3];  // forward F_D per stage
-    hlld_step_diag_t *diag;   // [3] forward sweep counters per stage
-    Scratch2D fw;             // forward work arrays
+    Scratch2D fw;
     double *lU0[6], *lBx0, *lBy0, *lBcx, *lBcy;
     double *lFx[NFLUX], *lFy[NFLUX], *lEz;
     double *lamS[kMaxNW * 7], *lamBn;
@@ -692,55 +704,79 @@ struct AdjScratch {
 
 static size_t adj_align(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// Carves the adjoint scratch out of base (NULL: size only).
-static size_t adjoint_layout(const hlld_grid2d_t *g, char *base, AdjScratch *sc) {
+struct Carver {
+    char *base;
+    size_t off = 0;
+    double *d(size_t n) {
+        double *p = base ? (double *)(base + off) : nullptr;
+        off += adj_align(n * 8);
+        return p;
+    }
+    uint8_t *b(size_t n) {
+        uint8_t *p = base ? (uint8_t *)(base + off) : nullptr;
+        off += adj_align(n);
+        return p;
+    }
+};
+
+static size_t tape_layout(const hlld_grid2d_t *g, char *base, AdjTape *t) {
+    const size_t nxt = g->nx + 2 * g->ng, nyt = g->ny + 2 * g->ng;
+    const size_t nfx = (nxt + 1) * nyt, nfy = nxt * (nyt + 1), nc = nxt * nyt;
+    Carver c{base};
+    AdjTape s{};
+    for (int x = 0; x < 2; ++x) {
+        for (int k = 0; k < 6; ++k) s.X[x].U[k] = c.d(nc);
+        s.X[x].Bxf = c.d(nfx);
+        s.X[x].Byf = c.d(nfy);
+        for (int k = 0; k < 9; ++k) s.X[x].P[k] = c.d(nc);
+    }
+    for (int st = 0; st < 3; ++st) {
+        s.FxD[st] = c.d(nfx);
+        s.FyD[st] = c.d(nfy);
+        s.psx[st] = c.d(nfx);
+        s.psy[st] = c.d(nfy);
+        s.fx[st] = c.b(nfx);
+        s.fy[st] = c.b(nfy);
+        s.mu[st] = c.d(nc);
+    }
+    s.diag = base ? (hlld_step_diag_t *)(base + c.off) : nullptr;
+    c.off += adj_align(3 * sizeof(hlld_step_diag_t));
+    if (t) *t = s;
+    return c.off;
+}
+
+static size_t scratch_layout(const hlld_grid2d_t *g, char *base, AdjScratch *sc) {
     const size_t nxt = g->nx + 2 * g->ng, nyt = g->ny + 2 * g->ng;
     const size_t nfx = (nxt + 1) * nyt, nfy = nxt * (nyt + 1), ncr = (nxt + 1) * (nyt + 1),
                  nc = nxt * nyt, nfmax = nfx > nfy ? nfx : nfy;
     const int nw = 2 * (g->limiter == HLLD_LIM_MP7 ? 3
                         : (g->limiter == HLLD_LIM_WENO5Z || g->limiter == HLLD_LIM_MP5) ? 2 : 1) + 2;
-    size_t off = 0;
-    auto take = [&](size_t count) -> double * {
-        double *p = base ? (double *)(base + off) : nullptr;
-        off += adj_align(count * 8);
-        return p;
-    };
+    Carver c{base};
     AdjScratch s{};
-    for (int x = 0; x < 2; ++x) {
-        for (int k = 0; k < 6; ++k) s.X[x].U[k] = take(nc);
-        s.X[x].Bxf = take(nfx);
-        s.X[x].Byf = take(nfy);
-        for (int k = 0; k < 9; ++k) s.X[x].P[k] = take(nc);
-    }
-    for (int st = 0; st < 3; ++st) {
-        s.FxD[st] = take(nfx);
-        s.FyD[st] = take(nfy);
-    }
-    s.diag = base ? (hlld_step_diag_t *)(base + off) : nullptr;
-    off += adj_align(3 * sizeof(hlld_step_diag_t));
-    for (int k = 0; k < 7; ++k) s.fw.Fx[k] = take(nfx);
-    for (int k = 0; k < 7; ++k) s.fw.Fy[k] = take(nfy);
-    s.fw.Ez = take(ncr);
-    for (int k = 0; k < 6; ++k) s.fw.U0[k] = take(nc);
-    s.fw.Bx0 = take(nfx);
-    s.fw.By0 = take(nfy);
+    for (int k = 0; k < 7; ++k) s.fw.Fx[k] = c.d(nfx);
+    for (int k = 0; k < 7; ++k) s.fw.Fy[k] = c.d(nfy);
+    s.fw.Ez = c.d(ncr);
+    for (int k = 0; k < 6; ++k) s.fw.U0[k] = c.d(nc);
+    s.fw.Bx0 = c.d(nfx);
+    s.fw.By0 = c.d(nfy);
     s.fw.diag = nullptr;
-    for (int k = 0; k < 6; ++k) s.lU0[k] = take(nc);
-    s.lBx0 = take(nfx);
-    s.lBy0 = take(nfy);
-    s.lBcx = take(nc);
-    s.lBcy = take(nc);
-    for (int k = 0; k < NFLUX; ++k) s.lFx[k] = take(nfx);
-    for (int k = 0; k < NFLUX; ++k) s.lFy[k] = take(nfy);
-    s.lEz = take(ncr);
+    for (int k = 0; k < 6; ++k) s.lU0[k] = c.d(nc);
+    s.lBx0 = c.d(nfx);
+    s.lBy0 = c.d(nfy);
+    s.lBcx = c.d(nc);
+    s.lBcy = c.d(nc);
+    for (int k = 0; k < NFLUX; ++k) s.lFx[k] = c.d(nfx);
+    for (int k = 0; k < NFLUX; ++k) s.lFy[k] = c.d(nfy);
+    s.lEz = c.d(ncr);
     // window-slot lambdas: only the limiter's window width is stored
-    for (int k = 0; k < kMaxNW * 7; ++k) s.lamS[k] = (k < nw * 7) ? take(nfmax) : nullptr;
-    s.lamBn = take(nfmax);
+    for (int k = 0; k < kMaxNW * 7; ++k) s.lamS[k] = (k < nw * 7) ? c.d(nfmax) : nullptr;
+    s.lamBn = c.d(nfmax);
     if (sc) *sc = s;
-    return off;
+    return c.off;
 }
 
-size_t adjoint_scratch_bytes(const hlld_grid2d_t *g) { return adjoint_layout(g, nullptr, nullptr); }
+size_t adjoint_tape_bytes(const hlld_grid2d_t *g) { return tape_layout(g, nullptr, nullptr); }
+size_t adjoint_reverse_scratch_bytes(const hlld_grid2d_t *g) { return scratch_layout(g, nullptr, nullptr); }
 
 void launch_prim_to_cons_vjp(int64_t n, const void *const *prim, const void *const *lam_cons,
                              void *const *lam_prim, cudaStream_t st) {
@@ -783,7 +819,8 @@ static void adj_fold(const GhostParams<double> &gp, int narr, cudaStream_t st) {
 // ghosts) at state X: lambda(P) -> lambda(U, faces); also moves the pending
 // cell-centred-B lambdas onto the faces
 static void adj_sync(const Grid &G, const AdjState &X, double *const *lU, double *lBxf, double *lByf,
-                     double *const *lP, const AdjScratch &sc, cudaStream_t st) {
+                     double *const *lP, const AdjScratch &sc, cudaStream_t st,
+                     const double *mu = nullptr) {
     // a. primitive ghosts
     adj_fold(ghost_params_cc(G, lP, 9), 9, st);
     // b. C2P of the physical cells
@@ -796,6 +833,7 @@ static void adj_sync(const Grid &G, const AdjState &X, double *const *lU, double
     for (int k = 0; k < 6; ++k) cp.lU[k] = lU[k];
     cp.lBcx = sc.lBcx;
     cp.lBcy = sc.lBcy;
+    cp.mu_in = mu;
     adj_c2p_kernel<<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(cp);
     // c. cell-centred B -> faces
     AdjBcParams bp = {G, sc.lBcx, sc.lBcy, lBxf, lByf};
@@ -872,44 +910,47 @@ static void copy_state(const Grid &G, const AdjState &src, const AdjState &dst, 
     cudaMemcpyAsync(dst.Byf, src.Byf, sizeof(double) * G.nxt * (G.nyt + 1), cudaMemcpyDeviceToDevice, st);
 }
 
-// s_in: the step's input state; s_out: its output (the forward step of s_in
-// with dt); lam: on entry lambda of the output (cons, faces, prims), on
-// return lambda of the input (prims lambda zero).
-void launch_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
-                               const hlld_state2d_t *s_out, double dt, int scheme,
-                               const hlld_state2d_t *lam, void *scratch, cudaStream_t st) {
+// One forward step (the same kernels and order as launch_rk_step_ct) that
+// advances s in place and records the tape.
+void launch_adjoint_record(const hlld_grid2d_t *g, const hlld_state2d_t *s, double dt, int scheme,
+                           void *tape, void *scratch, cudaStream_t st) {
     Grid G = make_grid(g);
+    AdjTape tp;
+    tape_layout(g, (char *)tape, &tp);
     AdjScratch sc;
-    adjoint_layout(g, (char *)scratch, &sc);
+    scratch_layout(g, (char *)scratch, &sc);
+    const int nst = scheme == 3 ? 3 : 2;
+    const size_t nfx = (size_t)(G.nxt + 1) * G.nyt, nfy = (size_t)G.nxt * (G.nyt + 1);
+    cudaMemsetAsync(tp.diag, 0, 3 * sizeof(hlld_step_diag_t), st);
+    const AdjState S = from_state(s);
+    for (int stage = 0; stage < nst; ++stage) {
+        hlld_step_diag_t *dg = tp.diag + stage;
+        ::hlld::v_fp64::launch_sweep2d(g, s, 0, sc.fw.Fx, &dg->sweep[0], st, tp.psx[stage], tp.fx[stage]);
+        ::hlld::v_fp64::launch_sweep2d(g, s, 1, sc.fw.Fy, &dg->sweep[1], st, tp.psy[stage], tp.fy[stage]);
+        cudaMemcpyAsync(tp.FxD[stage], sc.fw.Fx[F_D], sizeof(double) * nfx, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(tp.FyD[stage], sc.fw.Fy[F_D], sizeof(double) * nfy, cudaMemcpyDeviceToDevice, st);
+        ::hlld::v_fp64::launch_ct_update2d(g, s, sc.fw, dg, stage, scheme, dt, nullptr, st);
+        ::hlld::v_fp64::launch_sync_state(g, s, nullptr, dg, st, tp.mu[stage]);
+        if (stage + 1 < nst) copy_state(G, S, tp.X[stage], st);
+    }
+}
+
+// The reverse of one recorded step: s_in / s_out are the step's input and
+// output; lam: on entry lambda of the output (cons, faces, prims), on return
+// lambda of the input (prims lambda zero).
+void launch_adjoint_reverse(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
+                            const hlld_state2d_t *s_out, double dt, int scheme, const void *tape,
+                            const hlld_state2d_t *lam, void *scratch, cudaStream_t st) {
+    Grid G = make_grid(g);
+    AdjTape tp;
+    tape_layout(g, (char *)tape, &tp);
+    AdjScratch sc;
+    scratch_layout(g, (char *)scratch, &sc);
     const int nst = scheme == 3 ? 3 : 2;
     const size_t nc = (size_t)G.nxt * G.nyt, nfx = (size_t)(G.nxt + 1) * G.nyt,
                  nfy = (size_t)G.nxt * (G.nyt + 1);
-    // forward stages: X[0] = X_1, X[1] = X_2 (RK3); F_D and sweep counters
-    // of every stage
-    cudaMemsetAsync(sc.diag, 0, 3 * sizeof(hlld_step_diag_t), st);
     const AdjState X0 = from_state(s_in);
-    copy_state(G, X0, sc.X[0], st);
-    const AdjState Xs[3] = {X0, sc.X[0], sc.X[1]};
-    for (int stage = 0; stage < nst; ++stage) {
-        // stage 0 sweeps X[0] (a copy of X_0) and advances it to X_1;
-        // stage 1 sweeps X_1 and advances a copy of it in X[1] to X_2
-        const AdjState &Sw = stage == 0 ? sc.X[0] : Xs[stage];
-        hlld_state2d_t sweep_in = as_state(Sw);
-        hlld_step_diag_t *dg = sc.diag + stage;
-        ::hlld::v_fp64::launch_sweep2d(g, &sweep_in, 0, sc.fw.Fx, &dg->sweep[0], st);
-        ::hlld::v_fp64::launch_sweep2d(g, &sweep_in, 1, sc.fw.Fy, &dg->sweep[1], st);
-        cudaMemcpyAsync(sc.FxD[stage], sc.fw.Fx[F_D], sizeof(double) * nfx, cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(sc.FyD[stage], sc.fw.Fy[F_D], sizeof(double) * nfy, cudaMemcpyDeviceToDevice, st);
-        if (stage == nst - 1) break;
-        hlld_state2d_t work = sweep_in;
-        if (stage == 1) {
-            copy_state(G, Sw, sc.X[1], st);
-            work = as_state(sc.X[1]);
-        }
-        ::hlld::v_fp64::launch_ct_update2d(g, &work, sc.fw, dg, stage, scheme, dt, nullptr, st);
-        ::hlld::v_fp64::launch_sync_state(g, &work, nullptr, nullptr, st);
-    }
-    // reverse
+    const AdjState Xs[3] = {X0, tp.X[0], tp.X[1]};
     double *lU[6], *lP[9];
     for (int k = 0; k < 6; ++k) lU[k] = (double *)lam->cons[k];
     for (int k = 0; k < 9; ++k) lP[k] = (double *)lam->prims[k];
@@ -929,7 +970,7 @@ void launch_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_i
         const AdjState &Xout = stage == nst - 1 ? Xlast : Xs[stage + 1];
         const double *w = scheme == 3 ? kW3[stage] : kW2[stage];
         // a-d: lambda(P_{s+1}) -> lambda(U_{s+1}, faces_{s+1})
-        adj_sync(G, Xout, lU, lBxf, lByf, lP, sc, st);
+        adj_sync(G, Xout, lU, lBxf, lByf, lP, sc, st, tp.mu[stage]);
         // e: RK combine, divergence and CT curl
         AdjUpdateParams up = {};
         up.g = G;
@@ -958,9 +999,9 @@ void launch_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_i
         ep.vy = Xin.P[P_VY];
         ep.Bxf = Xin.Bxf;
         ep.Byf = Xin.Byf;
-        ep.FxD = sc.FxD[stage];
-        ep.FyD = sc.FyD[stage];
-        ep.diag = sc.diag + stage;
+        ep.FxD = tp.FxD[stage];
+        ep.FyD = tp.FyD[stage];
+        ep.diag = tp.diag + stage;
         ep.upwind = g->upwind;
         ep.lEz = sc.lEz;
         ep.lFxBt = sc.lFx[F_BT];
@@ -983,6 +1024,8 @@ void launch_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_i
             ap.Bxf = Xin.Bxf;
             ap.Byf = Xin.Byf;
             for (int k = 0; k < NFLUX; ++k) ap.lamF[k] = axis == 0 ? sc.lFx[k] : sc.lFy[k];
+            ap.pstar_in = axis == 0 ? tp.psx[stage] : tp.psy[stage];
+            ap.fail_in = axis == 0 ? tp.fx[stage] : tp.fy[stage];
             for (int k = 0; k < kMaxNW * 7; ++k) ap.lamS[k] = sc.lamS[k];
             ap.lamBn = sc.lamBn;
             AdjGatherParams gp = {};
@@ -1020,6 +1063,39 @@ void launch_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_i
     af.n = (int64_t)nfy;
     add_arrays_kernel<<<dim3(grid1d(af.n), 1), kThreads, 0, st>>>(af);
     adj_sync(G, X0, lU, lBxf, lByf, lP, sc, st);
+}
+
+// Self-contained form: the scratch holds the reverse's work arrays, a tape
+// and a working copy of s_in, which the recording step advances.
+static size_t state_layout(const hlld_grid2d_t *g, char *base, AdjState *X) {
+    const size_t nxt = g->nx + 2 * g->ng, nyt = g->ny + 2 * g->ng;
+    Carver c{base};
+    AdjState s{};
+    for (int k = 0; k < 6; ++k) s.U[k] = c.d(nxt * nyt);
+    s.Bxf = c.d((nxt + 1) * nyt);
+    s.Byf = c.d(nxt * (nyt + 1));
+    for (int k = 0; k < 9; ++k) s.P[k] = c.d(nxt * nyt);
+    if (X) *X = s;
+    return c.off;
+}
+
+size_t adjoint_scratch_bytes(const hlld_grid2d_t *g) {
+    return scratch_layout(g, nullptr, nullptr) + tape_layout(g, nullptr, nullptr) +
+           state_layout(g, nullptr, nullptr);
+}
+
+void launch_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
+                               const hlld_state2d_t *s_out, double dt, int scheme,
+                               const hlld_state2d_t *lam, void *scratch, cudaStream_t st) {
+    Grid G = make_grid(g);
+    char *tape = (char *)scratch + scratch_layout(g, nullptr, nullptr);
+    char *work = tape + tape_layout(g, nullptr, nullptr);
+    AdjState W;
+    state_layout(g, work, &W);
+    copy_state(G, from_state(s_in), W, st);
+    hlld_state2d_t ws = as_state(W);
+    launch_adjoint_record(g, &ws, dt, scheme, tape, scratch, st);
+    launch_adjoint_reverse(g, s_in, s_out, dt, scheme, tape, lam, scratch, st);
 }
 
 }  // namespace HLLD_NS

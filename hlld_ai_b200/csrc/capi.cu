@@ -359,6 +359,66 @@ int hlld_adjoint_scratch_bytes(const hlld_grid2d_t *g, size_t *bytes) {
     return HLLD_OK;
 }
 
+static int check_adjoint_grid(const hlld_grid2d_t *g) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (g->precision != HLLD_FP64)
+        return fail(HLLD_ERR_UNSUPPORTED, "the adjoint is implemented for HLLD_FP64");
+    if (g->solver == HLLD_SOLVER_HLLC)
+        return fail(HLLD_ERR_UNSUPPORTED, "the adjoint is implemented for HLLE and HLLD");
+    return HLLD_OK;
+}
+
+static int check_buffer(const void *p, size_t have, size_t need, const char *what) {
+    if (!p) return fail(HLLD_ERR_INVALID, "%s is NULL", what);
+    if ((uintptr_t)p % kAlign) return fail(HLLD_ERR_INVALID, "%s must be 256-byte aligned", what);
+    if (have < need) return fail(HLLD_ERR_SCRATCH, "%s has %zu bytes, %zu needed", what, have, need);
+    return HLLD_OK;
+}
+
+int hlld_adjoint_tape_bytes(const hlld_grid2d_t *g, size_t *tape_bytes, size_t *scratch_bytes) {
+    int rc = check_adjoint_grid(g);
+    if (rc) return rc;
+    if (!tape_bytes || !scratch_bytes) return fail(HLLD_ERR_INVALID, "size outputs are NULL");
+    *tape_bytes = hlld::v_adj::adjoint_tape_bytes(g);
+    *scratch_bytes = hlld::v_adj::adjoint_reverse_scratch_bytes(g);
+    return HLLD_OK;
+}
+
+int hlld_adjoint_record_step(const hlld_grid2d_t *g, const hlld_state2d_t *s, double dt,
+                             int scheme, void *tape, size_t tape_bytes, void *scratch,
+                             size_t scratch_bytes, void *stream) {
+    int rc = check_adjoint_grid(g);
+    if (rc) return rc;
+    if ((rc = check_state(s))) return rc;
+    if (scheme != 2 && scheme != 3) return fail(HLLD_ERR_INVALID, "scheme must be 2 or 3");
+    if (!(dt > 0.0)) return fail(HLLD_ERR_INVALID, "dt must be > 0");
+    if ((rc = check_buffer(tape, tape_bytes, hlld::v_adj::adjoint_tape_bytes(g), "tape"))) return rc;
+    if ((rc = check_buffer(scratch, scratch_bytes, hlld::v_adj::adjoint_reverse_scratch_bytes(g),
+                           "scratch")))
+        return rc;
+    hlld::v_adj::launch_adjoint_record(g, s, dt, scheme, tape, scratch, (cudaStream_t)stream);
+    return check_launch("adjoint_record_step");
+}
+
+int hlld_adjoint_reverse_step(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
+                              const hlld_state2d_t *s_out, double dt, int scheme, const void *tape,
+                              size_t tape_bytes, const hlld_state2d_t *lam, void *scratch,
+                              size_t scratch_bytes, void *stream) {
+    int rc = check_adjoint_grid(g);
+    if (rc) return rc;
+    if ((rc = check_state(s_in)) || (rc = check_state(s_out)) || (rc = check_state(lam))) return rc;
+    if (scheme != 2 && scheme != 3) return fail(HLLD_ERR_INVALID, "scheme must be 2 or 3");
+    if (!(dt > 0.0)) return fail(HLLD_ERR_INVALID, "dt must be > 0");
+    if ((rc = check_buffer(tape, tape_bytes, hlld::v_adj::adjoint_tape_bytes(g), "tape"))) return rc;
+    if ((rc = check_buffer(scratch, scratch_bytes, hlld::v_adj::adjoint_reverse_scratch_bytes(g),
+                           "scratch")))
+        return rc;
+    hlld::v_adj::launch_adjoint_reverse(g, s_in, s_out, dt, scheme, tape, lam, scratch,
+                                        (cudaStream_t)stream);
+    return check_launch("adjoint_reverse_step");
+}
+
 int hlld_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
                             const hlld_state2d_t *s_out, double dt, int scheme,
                             const hlld_state2d_t *lam, void *scratch, size_t scratch_bytes,

@@ -337,6 +337,9 @@ struct SweepParams {
     const double *Bxf, *Byf;
     R *F[NFLUX];
     hlld_flux_diag_t *diag;
+    // optional per-face record for the adjoint: p* and the HLLE fallback
+    double *pstar_out;
+    uint8_t *fail_out;
 };
 
 // One face of a directional sweep.  AXIS 0: faces (nxt+1, nyt), face f is
@@ -471,6 +474,10 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         p.F[F_TAU][fi] = o.F[C_TAU];
         p.F[F_BZ][fi] = o.F[C_BZ];
         p.F[F_BT][fi] = AXIS == 0 ? o.F[C_BY] : o.F[C_BX];
+        if (p.pstar_out) {
+            p.pstar_out[fi] = (double)o.pstar;
+            p.fail_out[fi] = (o.flags & RF_FAILED) ? 1 : 0;
+        }
         cnt.v[0] = 1;
         cnt.v[1] = o.err > 0;
         cnt.v[2] = (o.flags & RF_WAVE_ORDER_BAD) != 0;
@@ -696,6 +703,7 @@ struct C2PCellsParams {
     R *P[9];
     uint8_t *status;
     hlld_step_diag_t *diag;
+    double *mu_out;  // optional per-cell record of the C2P root (for the adjoint)
 };
 
 // cell-centred B (ct.py:44-54) + C2P (c2p.py:313-363) of the physical cells,
@@ -712,7 +720,9 @@ __global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParam
         double Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
         double C[NCONS] = {p.U[0][c], p.U[1][c], p.U[2][c], p.U[3][c], p.U[4][c], Bcx, Bcy, p.U[5][c]};
         double P[NPRIM];
-        uint8_t st = cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P);
+        double mu = 0.0;
+        uint8_t st = cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P, p.mu_out ? &mu : nullptr);
+        if (p.mu_out) p.mu_out[c] = mu;
 #pragma unroll
         for (int k = 0; k < NPRIM; ++k) p.P[k][c] = (R)P[k];
         if (p.status) p.status[c] = st;
@@ -1250,7 +1260,7 @@ static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStre
 }
 
 void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
-                       hlld_step_diag_t *diag, cudaStream_t st) {
+                       hlld_step_diag_t *diag, cudaStream_t st, double *mu_out) {
     Grid G = make_grid(g);
     double *cons[6];
     for (int k = 0; k < 6; ++k) cons[k] = (double *)s->cons[k];
@@ -1266,13 +1276,16 @@ void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t 
     for (int k = 0; k < 9; ++k) cp.P[k] = prims[k];
     cp.status = status;
     cp.diag = diag;
+    cp.mu_out = mu_out;
     c2p_cells_kernel<<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(cp);
     launch_ghost_cc<R>(G, prims, 9, st);
 }
 
 void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
-                    hlld_flux_diag_t *fdiag, cudaStream_t st) {
+                    hlld_flux_diag_t *fdiag, cudaStream_t st, double *pstar_out, uint8_t *fail_out) {
     SweepParams sp = {};
+    sp.pstar_out = pstar_out;
+    sp.fail_out = fail_out;
     sp.g = make_grid(g);
     sp.rho = (const R *)s->prims[P_RHO];
     sp.p = (const R *)s->prims[P_P];

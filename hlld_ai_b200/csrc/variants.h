@@ -33,14 +33,15 @@ struct Scratch2D {
     void launch_prim_to_cons(int64_t n, const void *const *prim, void *const *cons,               \
                              cudaStream_t st);                                                    \
     void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,      \
-                           hlld_step_diag_t *diag, cudaStream_t st);                              \
+                           hlld_step_diag_t *diag, cudaStream_t st, double *mu_out = nullptr);    \
     void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,  \
                            double dt_host, const double *dt_dev, int scheme,                      \
                            hlld_step_diag_t *diag, cudaStream_t st);                              \
     void launch_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,        \
                               double *dt_dev, unsigned long long *work, cudaStream_t st);         \
     void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis,                \
-                        void *const *F, hlld_flux_diag_t *fdiag, cudaStream_t st);                \
+                        void *const *F, hlld_flux_diag_t *fdiag, cudaStream_t st,                 \
+                        double *pstar_out = nullptr, uint8_t *fail_out = nullptr);                \
     void launch_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,           \
                           void *const *U0, void *const *F, double *t_out, int32_t *steps_out,     \
                           unsigned int *next, int threads, int blocks, cudaStream_t st);          \
@@ -55,6 +56,13 @@ int report_error(int code, const char *fmt, ...);
 HLLD_DECLARE_VARIANT(v_fp64)
 namespace v_adj {  // the discrete adjoint of the FP64 step (adjoint_fp64.cu)
 size_t adjoint_scratch_bytes(const hlld_grid2d_t *g);
+size_t adjoint_tape_bytes(const hlld_grid2d_t *g);
+size_t adjoint_reverse_scratch_bytes(const hlld_grid2d_t *g);
+void launch_adjoint_record(const hlld_grid2d_t *g, const hlld_state2d_t *s, double dt, int scheme,
+                           void *tape, void *scratch, cudaStream_t st);
+void launch_adjoint_reverse(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
+                            const hlld_state2d_t *s_out, double dt, int scheme, const void *tape,
+                            const hlld_state2d_t *lam, void *scratch, cudaStream_t st);
 void launch_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
                                const hlld_state2d_t *s_out, double dt, int scheme,
                                const hlld_state2d_t *lam, void *scratch, cudaStream_t st);

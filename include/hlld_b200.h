@@ -251,6 +251,24 @@ int hlld_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
                    void *const *U0, void *const *F, double *t_out, int32_t *steps_out,
                    unsigned int *next, int threads, int blocks, void *stream);
 
+/* The adjoint split in two, for checkpointed runs that recompute a segment
+ * once: hlld_adjoint_record_step advances s by one step exactly as
+ * hlld_rk_step_ct does and writes the step's tape (the stage-1 and stage-2
+ * inputs and, per stage, F_D, the sweep counters and each face's p* and
+ * HLLE fallback); hlld_adjoint_reverse_step then maps lambda of the output
+ * to lambda of the input without recomputing the forward.  Sizes from
+ * hlld_adjoint_tape_bytes (one tape per recorded step; the scratch can be
+ * shared by all calls on one stream).  No counterpart in the reference.
+ * FP64, HLLE or HLLD; buffers 256-byte aligned. */
+int hlld_adjoint_tape_bytes(const hlld_grid2d_t *g, size_t *tape_bytes, size_t *scratch_bytes);
+int hlld_adjoint_record_step(const hlld_grid2d_t *g, const hlld_state2d_t *s, double dt,
+                             int scheme, void *tape, size_t tape_bytes, void *scratch,
+                             size_t scratch_bytes, void *stream);
+int hlld_adjoint_reverse_step(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
+                              const hlld_state2d_t *s_out, double dt, int scheme, const void *tape,
+                              size_t tape_bytes, const hlld_state2d_t *lam, void *scratch,
+                              size_t scratch_bytes, void *stream);
+
 /* Reverse of src/physics/hlld.py:185-217 primitive_to_conserved on n
  * elements (FP64): lam_prim[9] = (d cons / d prim)^T lam_cons[8], with eps
  * an independent input as it is there.  Entries of lam_cons may be NULL

@@ -195,3 +195,29 @@ def test_rotor_gradient_study_small():
     assert r1["J"] == r2["J"]
     assert r1["grad_omega"] == r2["grad_omega"]
     assert torch.equal(r1["grad_rho0"], r2["grad_rho0"])
+
+
+def test_recorded_step_and_reverse_match_the_self_contained_adjoint():
+    """hlld_adjoint_record_step advances the state exactly as the production
+    step does, and the reverse from its tape equals hlld_adjoint_rk_step_ct
+    (which records internally) bit for bit."""
+    g, eos, st, run = smooth_random_state(24, "mc", seed=5)
+    dt = float(run.stepper.compute_dt(st, 0.4).item())
+    a, b = st.clone(), st.clone()
+    run.stepper.step(a, dt, "rk3")
+    run.record_step(b, dt, 0)
+    for k in EVOLVED_KEYS:
+        assert torch.equal(a.cons[k], b.cons[k]), k
+    assert torch.equal(a.Bxf, b.Bxf) and torch.equal(a.Byf, b.Byf)
+    from hlld_ai_b200.adjoint import _zeros_state
+    gen = torch.Generator(device="cuda").manual_seed(2)
+    lam1 = _zeros_state(g, "cuda")
+    for k in EVOLVED_KEYS:
+        lam1.cons[k][g.phys] = torch.rand(lam1.cons[k][g.phys].shape, generator=gen, device="cuda",
+                                          dtype=torch.float64)
+    lam2 = lam1.clone()
+    run.reverse_step(st, b, dt, 0, lam1)
+    run.step_adjoint(st, a, dt, lam2)
+    for k in EVOLVED_KEYS:
+        assert torch.equal(lam1.cons[k], lam2.cons[k]), k
+    assert torch.equal(lam1.Bxf, lam2.Bxf) and torch.equal(lam1.Byf, lam2.Byf)
