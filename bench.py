@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--cpu-n", type=int, default=512, help="grid of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint/forward cost of the 512^2 rotor gradient study")
     ap.add_argument("--workload", default="rotor", choices=["rotor", "tubes"],
                     help="rotor: the 2D rotor step (default); tubes: the batched-tube launch")
     ap.add_argument("--tubes", type=int, default=4096)
@@ -401,6 +403,22 @@ def run_ours(a):
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "steps": ke, "path": "Stepper2D.step + compute_dt with pinned host state"}
 
+    # the adjoint's cost against the forward (the rotor gradient study: 512^2,
+    # 200 FP64 SSP-RK3 steps, checkpoints every 20, J = sum w |B|^2 / 2)
+    adj = None
+    if not a.no_adjoint:
+        from hlld_ai_b200.adjoint import RotorCase, rotor_gradients
+
+        torch.cuda.empty_cache()
+        r = rotor_gradients(RotorCase(n=512, steps=200, checkpoint_every=20), device=dev)
+        adj = {"workload": "rotor 512^2, FP64 HLLD + PLM(MC) + CT, 200 SSP-RK3 steps, "
+                           "checkpoint every 20, J = sum w |B_c|^2 / 2",
+               "forward_ms": r["forward_ms"], "adjoint_ms": r["adjoint_ms"],
+               "adjoint_over_forward": r["adjoint_ms"] / r["forward_ms"],
+               "J": r["J"], "dJ_domega": r["grad_omega"]}
+        del r
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -421,6 +439,7 @@ def run_ours(a):
                        "parallelism": f"replicas x{world}", "cfl": a.cfl,
                        "l2": "inputs exceed L2 (state >1 GB at 2048^2), no flush"},
             "fp64": fp64_arm,
+            "adjoint": adj,
             "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps,
             "roofline": {"bound": "hbm", "kernel": "sweep_kernel (x and y)",
