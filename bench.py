@@ -213,6 +213,8 @@ def _timed_rotor(a, precision, dev, world, record=True):
     U0 = [torch.empty(g.nxt * g.nyt, **f64) for _ in range(6)]
     Bx0, By0 = torch.empty(nfx, **f64), torch.empty(nfy, **f64)
     diag = torch.zeros(ctypes.sizeof(_lib.StepDiag), dtype=torch.uint8, device=dev)
+    # the mixed form's C2P roots of the step's first stage (as hlld_rk_step_ct)
+    mu = torch.zeros(g.nxt * g.nyt, dtype=torch.float64, device=dev) if precision == "mixed" else None
     fd_off = ctypes.sizeof(_lib.FluxDiag)
     pFx, pFy, pU0 = _lib.ptr_array(Fx), _lib.ptr_array(Fy), _lib.ptr_array(U0)
     dt = stepper.dt_buf
@@ -235,8 +237,14 @@ def _timed_rotor(a, precision, dev, world, record=True):
                                           Ez.data_ptr(), pU0, Bx0.data_ptr(), By0.data_ptr(),
                                           diag.data_ptr(), stage, 3, 0.0, dt.data_ptr(), sh),
                        "ct_update2d")
-            _lib.check(L.hlld_sync_state(ctypes.byref(gc), ctypes.byref(s), None, None, sh),
-                       "sync_state")
+            if mu is None:
+                _lib.check(L.hlld_sync_state(ctypes.byref(gc), ctypes.byref(s), None, None, sh),
+                           "sync_state")
+            else:
+                _lib.check(L.hlld_sync_state_roots(ctypes.byref(gc), ctypes.byref(s), None, None,
+                                                   mu.data_ptr() if stage == 0 else None,
+                                                   None if stage == 0 else mu.data_ptr(), sh),
+                           "sync_state_roots")
 
     for _ in range(a.warmup):
         step()

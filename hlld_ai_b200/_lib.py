@@ -88,6 +88,8 @@ SIGNATURES = {
                                               ctypes.c_double, _VP, ctypes.c_int, _VP, _VP]),
     "hlld_sync_state": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC), _VP,
                                        _VP, _VP]),
+    "hlld_sync_state_roots": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
+                                             _VP, _VP, _VP, _VP, _VP]),
     "hlld_sweep2d": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
                                     ctypes.c_int, _PP, _VP, _VP]),
     "hlld_ct_update2d": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC), _PP,

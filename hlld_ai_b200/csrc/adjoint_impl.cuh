@@ -375,13 +375,37 @@ __global__ void __launch_bounds__(kThreads) adj_bc_faces_kernel(const AdjBcParam
 // Every entry of the never-written block adds the lambdas of the ghost
 // entries filled from it (a gather, so the sum order is fixed).  The ghost
 // indices of each axis are [0, a) and [b, n): at most 2 ng + 1 of them.
+// Only the band within ng + 1 of the block's edges can be a source; the
+// threads enumerate that band (the block minus its inner hole).
+__host__ __device__ __forceinline__ int fold_band(const int ng) { return ng + 1; }
+__host__ __device__ __forceinline__ int fold_hole(int in, int band) {
+    return in > 2 * band ? in - 2 * band : 0;
+}
+
 template <typename E>
 __global__ void __launch_bounds__(kThreads) adj_fold_kernel(const GhostParams<E> p) {
     E *v = p.v[blockIdx.y];
     const int in0 = p.b0 - p.a0, in1 = p.b1 - p.a1;
+    const int B = fold_band(p.ng);
+    int h0 = fold_hole(in0, B), h1 = fold_hole(in1, B);
+    if (h0 == 0 || h1 == 0) h0 = h1 = 0;
+    const int64_t nA = (int64_t)(in0 - h0) * in1;
+    const int64_t nB = (int64_t)h0 * (in1 - h1);
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (int64_t)in0 * in1) return;
-    const int r = p.a0 + (int)(e / in1), c = p.a1 + (int)(e % in1);
+    if (e >= nA + nB) return;
+    int rr, cc;
+    if (e < nA) {
+        const int q = (int)(e / in1);
+        cc = (int)(e - (int64_t)q * in1);
+        rr = (h0 > 0 && q >= B) ? q + h0 : q;
+    } else {
+        const int64_t e2 = e - nA;
+        const int w = in1 - h1;
+        const int q = (int)(e2 / w), k = (int)(e2 - (int64_t)q * w);
+        rr = B + q;
+        cc = k < B ? k : k + h1;
+    }
+    const int r = p.a0 + rr, c = p.a1 + cc;
     int rs[8], cs[8], nr = 1, nc = 1;
     rs[0] = r;
     cs[0] = c;
@@ -809,9 +833,14 @@ static GhostParams<double> ghost_params_cc(const Grid &G, double *const *arrs, i
 }
 
 static void adj_fold(const GhostParams<double> &gp, int narr, cudaStream_t st) {
-    const int64_t in = (int64_t)(gp.b0 - gp.a0) * (gp.b1 - gp.a1);
+    const int in0 = gp.b0 - gp.a0, in1 = gp.b1 - gp.a1;
+    const int64_t in = (int64_t)in0 * in1;
     const int64_t out = (int64_t)gp.n0 * gp.n1 - in;
-    adj_fold_kernel<double><<<dim3(grid1d(in), narr), kThreads, 0, st>>>(gp);
+    const int B = fold_band(gp.ng);
+    int h0 = fold_hole(in0, B), h1 = fold_hole(in1, B);
+    if (h0 == 0 || h1 == 0) h0 = h1 = 0;
+    const int64_t band = in - (int64_t)h0 * h1;
+    adj_fold_kernel<double><<<dim3(grid1d(band), narr), kThreads, 0, st>>>(gp);
     adj_zero_ghost_kernel<double><<<dim3(grid1d(out), narr), kThreads, 0, st>>>(gp);
 }
 

@@ -92,6 +92,8 @@ size_t layout_scratch(const hlld_grid2d_t *g, char *base, hlld::Scratch2D *sc) {
     s.By0 = (double *)take(nfy, 8);
     s.diag = base ? (hlld_step_diag_t *)(base + off) : nullptr;
     off += align_up(sizeof(hlld_step_diag_t));
+    // mixed form: the C2P roots of the step's first stage (warm start)
+    s.mu_warm = g->precision == HLLD_MIXED ? (double *)take(nc, 8) : nullptr;
     if (sc) *sc = s;
     return off;
 }
@@ -220,6 +222,25 @@ int hlld_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *st
     else
         hlld::v_fp64::launch_sync_state(g, s, status, diag, st);
     return check_launch("sync_state");
+}
+
+int hlld_sync_state_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
+                          hlld_step_diag_t *diag, double *mu_out, double *mu_start, void *stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_state(s))) return rc;
+    if (mu_start && g->precision != HLLD_MIXED)
+        return fail(HLLD_ERR_UNSUPPORTED, "the C2P warm start belongs to the mixed form");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (diag && cudaMemsetAsync(diag, 0, sizeof(hlld_step_diag_t), st) != cudaSuccess)
+        return check_launch("sync_state diag reset");
+    if (g->precision == HLLD_FP64_EXACT)
+        hlld::v_exact::launch_sync_state(g, s, status, diag, st, mu_out, nullptr);
+    else if (g->precision == HLLD_MIXED)
+        hlld::v_mixed::launch_sync_state(g, s, status, diag, st, mu_out, mu_start);
+    else
+        hlld::v_fp64::launch_sync_state(g, s, status, diag, st, mu_out, nullptr);
+    return check_launch("sync_state_roots");
 }
 
 int hlld_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,

@@ -704,6 +704,7 @@ struct C2PCellsParams {
     uint8_t *status;
     hlld_step_diag_t *diag;
     double *mu_out;  // optional per-cell record of the C2P root (for the adjoint)
+    double *mu_warm; // optional per-cell previous root, read as the start and updated
 };
 
 // cell-centred B (ct.py:44-54) + C2P (c2p.py:313-363) of the physical cells,
@@ -721,8 +722,11 @@ __global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParam
         double C[NCONS] = {p.U[0][c], p.U[1][c], p.U[2][c], p.U[3][c], p.U[4][c], Bcx, Bcy, p.U[5][c]};
         double P[NPRIM];
         double mu = 0.0;
-        uint8_t st = cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P, p.mu_out ? &mu : nullptr);
+        const double mu0 = p.mu_warm ? p.mu_warm[c] : 0.0;
+        uint8_t st = cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P,
+                                          (p.mu_out || p.mu_warm) ? &mu : nullptr, mu0);
         if (p.mu_out) p.mu_out[c] = mu;
+        if (p.mu_warm) p.mu_warm[c] = mu;
 #pragma unroll
         for (int k = 0; k < NPRIM; ++k) p.P[k][c] = (R)P[k];
         if (p.status) p.status[c] = st;
@@ -1260,7 +1264,7 @@ static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStre
 }
 
 void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
-                       hlld_step_diag_t *diag, cudaStream_t st, double *mu_out) {
+                       hlld_step_diag_t *diag, cudaStream_t st, double *mu_out, double *mu_warm) {
     Grid G = make_grid(g);
     double *cons[6];
     for (int k = 0; k < 6; ++k) cons[k] = (double *)s->cons[k];
@@ -1277,6 +1281,7 @@ void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t 
     cp.status = status;
     cp.diag = diag;
     cp.mu_out = mu_out;
+    cp.mu_warm = mu_warm;
     c2p_cells_kernel<<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(cp);
     launch_ghost_cc<R>(G, prims, 9, st);
 }
@@ -1358,7 +1363,11 @@ void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Sc
         launch_sweep2d(g, s, 0, sc.Fx, &diag->sweep[0], st);
         launch_sweep2d(g, s, 1, sc.Fy, &diag->sweep[1], st);
         launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
-        launch_sync_state(g, s, nullptr, diag, st);
+        // mixed form: stage 0 solves every cell's C2P in full and keeps the
+        // roots; the later stages of the step start from them (within the
+        // step only, so a step never depends on earlier calls)
+        if (stage == 0) launch_sync_state(g, s, nullptr, diag, st, sc.mu_warm, nullptr);
+        else launch_sync_state(g, s, nullptr, diag, st, nullptr, sc.mu_warm);
     }
 }
 

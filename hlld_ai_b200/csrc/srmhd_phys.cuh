@@ -425,19 +425,52 @@ __device__ __forceinline__ void kastaun_bisect(const Kastaun<T> &k, T mu_plus, C
 
 // c2p.py:313-363 conservative_to_primitive for one element; P gets the nine
 // primitives (B copied from C).
+// Warm start (used by the mixed-precision form only): a secant on the
+// master function from the previous root mu0 of the same cell.  It returns
+// false -- and the caller runs the full bracketed solve -- unless it reaches
+// |f| < tol within eight steps at a positive root.  The master function has
+// a single root in the physical interval (0, mu+], and a start next to it
+// converges to it.
+template <typename T>
+__device__ __forceinline__ bool kastaun_warm(const Kastaun<T> &k, T mu0, C2POut<T> &o) {
+    const T tol = K<T>::c2p_tol;
+    if (!(mu0 > T(0)) || !(mu0 < T(1e300))) return false;
+    T x0 = mu0 * (T(1) - T(1e-7)), x1 = mu0;
+    T f0 = k.master(x0), f1 = k.master(x1);
+#pragma unroll 1
+    for (int it = 0; it < 8; ++it) {
+        if (fabs(f1) < tol) {
+            if (!(x1 > T(0))) return false;
+            kastaun_finish(k, x1, true, true, o);
+            return true;
+        }
+        const T df = f1 - f0;
+        if (!(fabs(df) > T(1e-300))) return false;
+        const T x2 = x1 - f1 * (x1 - x0) / df;
+        if (!(x2 > T(0)) || !(x2 < T(1e300))) return false;
+        x0 = x1;
+        f0 = f1;
+        x1 = x2;
+        f1 = k.master(x1);
+    }
+    return false;
+}
+
 template <typename T>
 __device__ __forceinline__ uint8_t cons_to_prim(const T *C, T gamma, T atmo_rho, T atmo_eps,
-                                                T *P, T *mu_out = nullptr) {
+                                                T *P, T *mu_out = nullptr, T mu_warm = T(0)) {
     Kastaun<T> k;
     k.init(C, gamma);
-    T mp = k.mu_plus();
     C2POut<T> o;
-    kastaun_invert(k, mp, o);
     uint8_t extra = 0;
-    if (!(o.status & ST_CONVERGED) && (o.status & ST_BRACKET_OK)) {
-        kastaun_bisect(k, mp, o);
-        o.status |= ST_BRACKET_OK;
-        extra = ST_BISECTED;
+    if (!(mu_warm > T(0)) || !kastaun_warm(k, mu_warm, o)) {
+        T mp = k.mu_plus();
+        kastaun_invert(k, mp, o);
+        if (!(o.status & ST_CONVERGED) && (o.status & ST_BRACKET_OK)) {
+            kastaun_bisect(k, mp, o);
+            o.status |= ST_BRACKET_OK;
+            extra = ST_BISECTED;
+        }
     }
     if (mu_out) *mu_out = o.mu;
     T rho = o.rho, eps = o.eps, vx = o.v[0], vy = o.v[1], vz = o.v[2];

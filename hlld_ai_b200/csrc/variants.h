@@ -19,6 +19,7 @@ struct Scratch2D {
     double *U0[6];  // RK stage-0 copy of the evolved cell variables
     double *Bx0, *By0;
     hlld_step_diag_t *diag;  // used when the caller passes none
+    double *mu_warm;         // mixed form: each cell's last C2P root (warm start), or NULL
 };
 
 #define HLLD_DECLARE_VARIANT(NS)                                                                  \
@@ -33,7 +34,8 @@ struct Scratch2D {
     void launch_prim_to_cons(int64_t n, const void *const *prim, void *const *cons,               \
                              cudaStream_t st);                                                    \
     void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,      \
-                           hlld_step_diag_t *diag, cudaStream_t st, double *mu_out = nullptr);    \
+                           hlld_step_diag_t *diag, cudaStream_t st, double *mu_out = nullptr,     \
+                           double *mu_warm = nullptr);                                             \
     void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,  \
                            double dt_host, const double *dt_dev, int scheme,                      \
                            hlld_step_diag_t *diag, cudaStream_t st);                              \

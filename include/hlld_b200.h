@@ -212,6 +212,18 @@ int hlld_rk_step_ct_static(const hlld_grid2d_t *g, const hlld_state2d_t *s, doub
 int hlld_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
                     hlld_step_diag_t *diag, void *stream);
 
+/* hlld_sync_state that also exposes the C2P roots (device, nxt*nyt doubles,
+ * physical cells written): mu_out (may be NULL) receives each cell's root;
+ * mu_start (HLLD_MIXED only, may be NULL) holds a previous root of each cell
+ * to start the root search from, and is updated.  hlld_rk_step_ct does the
+ * same internally in the mixed form: its first stage solves every cell in
+ * full and its later stages start from those roots.  (The reference
+ * always solves from the bracket, c2p.py:188-236; a started search reaches
+ * the same |f| < 1e-15 root, and falls back to the bracketed solve if it does
+ * not within eight steps.) */
+int hlld_sync_state_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
+                          hlld_step_diag_t *diag, double *mu_out, double *mu_start, void *stream);
+
 /* Replaces src/physics/sweep.py:30-119 sweep() in the form the 2D step uses
  * it (reconstruct_prims, normal B taken from the staggered faces
  * sweep.py:82-89, flux_fn on every face, F[B_n] = 0 sweep.py:99-100), fused
