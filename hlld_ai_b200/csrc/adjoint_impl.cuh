@@ -74,70 +74,89 @@ __global__ void __launch_bounds__(kThreads) adj_sweep_kernel(const AdjSweepParam
         int c = f - 1 - S + k;
         cw[k] = c < 0 ? 0 : (c > n - 1 ? n - 1 : c);
     }
-    const int kedge = f == 0 ? S + 1 : S;  // slot of the edge cell on an outermost face
-    // work variables of the window (reconstruction.py:269)
-    double q[7][NW], vel[3][NW], Wf[NW];
-#pragma unroll
-    for (int k = 0; k < NW; ++k) {
+    // on an outermost face the edge cell sits in slot S + 1 (f = 0) or S (f = n)
+    // work variables of window slot k (reconstruction.py:269): rho, p, W v,
+    // B_t, Bz; velocities and W kept for the conversion's reverse
+    auto load_slot = [&](int k, double *qk, double *vk, double &W) {
         const int64_t ci = cbase + cw[k] * cstride;
-        vel[0][k] = p.vx[ci];
-        vel[1][k] = p.vy[ci];
-        vel[2][k] = p.vz[ci];
-        double v2 = vel[0][k] * vel[0][k] + vel[1][k] * vel[1][k] + vel[2][k] * vel[2][k];
-        Wf[k] = 1.0 / sqrt(clamp_lo(1.0 - v2, 1e-14));
-        q[0][k] = p.rho[ci];
-        q[1][k] = p.p[ci];
-        q[2][k] = Wf[k] * vel[0][k];
-        q[3][k] = Wf[k] * vel[1][k];
-        q[4][k] = Wf[k] * vel[2][k];
-        q[5][k] = bt_at(cw[k]);
-        q[6][k] = p.bz[ci];
-    }
-    double L[7], Rt[7];
-    bool bad = false;
-    if (edge) {
-#pragma unroll
-        for (int v = 0; v < 7; ++v) {
-            L[v] = q[v][kedge] + 0.5 * 0.0;
-            Rt[v] = q[v][kedge] - 0.5 * 0.0;
-        }
-    } else {
-#pragma unroll
-        for (int v = 0; v < 7; ++v) {
-            L[v] = cell_edge<LIM, true, S>(q[v], f - 1, n);
-            Rt[v] = cell_edge<LIM, false, S + 1>(q[v], f, n);
-        }
-        if (LIM != HLLD_LIM_PCM) {
-            bad = (L[0] <= 1e-12) || (Rt[0] <= 1e-12) || (L[1] <= 1e-14) || (Rt[1] <= 1e-14);
-            if (bad) {
-#pragma unroll
-                for (int v = 0; v < 7; ++v) {
-                    L[v] = q[v][S] + 0.5 * 0.0;
-                    Rt[v] = q[v][S + 1] - 0.5 * 0.0;
-                }
-            }
-        }
-    }
+        vk[0] = p.vx[ci];
+        vk[1] = p.vy[ci];
+        vk[2] = p.vz[ci];
+        double v2 = vk[0] * vk[0] + vk[1] * vk[1] + vk[2] * vk[2];
+        W = 1.0 / sqrt(clamp_lo(1.0 - v2, 1e-14));
+        qk[0] = p.rho[ci];
+        qk[1] = p.p[ci];
+        qk[2] = W * vk[0];
+        qk[3] = W * vk[1];
+        qk[4] = W * vk[2];
+        qk[5] = bt_at(cw[k]);
+        qk[6] = p.bz[ci];
+    };
     const double bn = AXIS == 0 ? p.Bxf[(int64_t)f * g.nyt + tr] : p.Byf[(int64_t)tr * (g.nyt + 1) + f];
     constexpr int IBT = AXIS == 0 ? P_BY : P_BX;
     constexpr int IBN = AXIS == 0 ? P_BX : P_BY;
-    // forward face states and the solved face
-    double PL[NPRIM], PR[NPRIM], fac[2];
+    // forward face states.  Only what the reverse of the conversion needs is
+    // kept through the Riemann solver's reverse (the face's W v, its
+    // 1/sqrt(1 + (W v)^2) and the floor flags); the window is loaded again
+    // afterwards for the reconstruction's reverse.
+    double PL[NPRIM], PR[NPRIM], fac[2], zq[2][3];
+    bool floor_rho[2], floor_p[2];
+    bool bad = false;
+    {
+        double q[7][NW];
 #pragma unroll
-    for (int side = 0; side < 2; ++side) {
-        const double *qq = side == 0 ? L : Rt;
-        double *P = side == 0 ? PL : PR;
-        double z2 = qq[2] * qq[2] + qq[3] * qq[3] + qq[4] * qq[4];
-        fac[side] = 1.0 / sqrt(1.0 + z2);
-        P[P_VX] = qq[2] * fac[side];
-        P[P_VY] = qq[3] * fac[side];
-        P[P_VZ] = qq[4] * fac[side];
-        P[P_RHO] = clamp_lo(qq[0], 1e-12);
-        P[P_P] = clamp_lo(qq[1], 1e-14);
-        P[P_EPS] = eos_eps(P[P_P], P[P_RHO], g.gamma);
-        P[IBN] = bn;
-        P[IBT] = qq[5];
-        P[P_BZ] = qq[6];
+        for (int k = 0; k < NW; ++k) {
+            double qk[7], vk[3], W;
+            load_slot(k, qk, vk, W);
+#pragma unroll
+            for (int v = 0; v < 7; ++v) q[v][k] = qk[v];
+        }
+        double L[7], Rt[7];
+        if (edge) {
+#pragma unroll
+            for (int v = 0; v < 7; ++v) {
+                const double x = f == 0 ? q[v][S + 1] : q[v][S];  // constant slots: registers
+                L[v] = x + 0.5 * 0.0;
+                Rt[v] = x - 0.5 * 0.0;
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 7; ++v) {
+                L[v] = cell_edge<LIM, true, S>(q[v], f - 1, n);
+                Rt[v] = cell_edge<LIM, false, S + 1>(q[v], f, n);
+            }
+            if (LIM != HLLD_LIM_PCM) {
+                bad = (L[0] <= 1e-12) || (Rt[0] <= 1e-12) || (L[1] <= 1e-14) || (Rt[1] <= 1e-14);
+                if (bad) {
+#pragma unroll
+                    for (int v = 0; v < 7; ++v) {
+                        L[v] = q[v][S] + 0.5 * 0.0;
+                        Rt[v] = q[v][S + 1] - 0.5 * 0.0;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const double *qq = side == 0 ? L : Rt;
+            double *P = side == 0 ? PL : PR;
+            double z2 = qq[2] * qq[2] + qq[3] * qq[3] + qq[4] * qq[4];
+            fac[side] = 1.0 / sqrt(1.0 + z2);
+            P[P_VX] = qq[2] * fac[side];
+            P[P_VY] = qq[3] * fac[side];
+            P[P_VZ] = qq[4] * fac[side];
+            P[P_RHO] = clamp_lo(qq[0], 1e-12);
+            P[P_P] = clamp_lo(qq[1], 1e-14);
+            P[P_EPS] = eos_eps(P[P_P], P[P_RHO], g.gamma);
+            P[IBN] = bn;
+            P[IBT] = qq[5];
+            P[P_BZ] = qq[6];
+            zq[side][0] = qq[2];
+            zq[side][1] = qq[3];
+            zq[side][2] = qq[4];
+            floor_rho[side] = qq[0] < 1e-12;
+            floor_p[side] = qq[1] < 1e-14;
+        }
     }
     double given[2] = {0.0, 0.0};
     if (SOLVER == HLLD_SOLVER_HLLD) {
@@ -183,16 +202,27 @@ __global__ void __launch_bounds__(kThreads) adj_sweep_kernel(const AdjSweepParam
     double lq[2][7];
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
-        const double *qq = side == 0 ? L : Rt;
         const double *l = lam + side * 7;
-        lq[side][0] = qq[0] < 1e-12 ? 0.0 : l[0];
-        lq[side][1] = qq[1] < 1e-14 ? 0.0 : l[1];
+        lq[side][0] = floor_rho[side] ? 0.0 : l[0];
+        lq[side][1] = floor_p[side] ? 0.0 : l[1];
         const double fc = fac[side], fc3 = fc * fc * fc;
-        const double zl = qq[2] * l[2] + qq[3] * l[3] + qq[4] * l[4];
+        const double zl = zq[side][0] * l[2] + zq[side][1] * l[3] + zq[side][2] * l[4];
 #pragma unroll
-        for (int j = 0; j < 3; ++j) lq[side][2 + j] = fc * l[2 + j] - fc3 * qq[2 + j] * zl;
+        for (int j = 0; j < 3; ++j) lq[side][2 + j] = fc * l[2 + j] - fc3 * zq[side][j] * zl;
         lq[side][5] = l[5];
         lq[side][6] = l[6];
+    }
+    // the window again (the store above may alias it for all the compiler
+    // knows, so these are fresh loads, not values held since the start)
+    double q[7][NW], vel[3][NW], Wf[NW];
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        double qk[7], vk[3];
+        load_slot(k, qk, vk, Wf[k]);
+#pragma unroll
+        for (int v = 0; v < 7; ++v) q[v][k] = qk[v];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) vel[j][k] = vk[j];
     }
     // reverse of the reconstruction onto the window slots
     double ls[7][NW];
@@ -202,7 +232,10 @@ __global__ void __launch_bounds__(kThreads) adj_sweep_kernel(const AdjSweepParam
         for (int k = 0; k < NW; ++k) ls[v][k] = 0.0;
     if (edge) {
 #pragma unroll
-        for (int v = 0; v < 7; ++v) ls[v][kedge] = lq[0][v] + lq[1][v];
+        for (int v = 0; v < 7; ++v) {
+            if (f == 0) ls[v][S + 1] = lq[0][v] + lq[1][v];
+            else ls[v][S] = lq[0][v] + lq[1][v];
+        }
     } else if (bad) {
 #pragma unroll
         for (int v = 0; v < 7; ++v) {

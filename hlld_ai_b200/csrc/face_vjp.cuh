@@ -241,13 +241,60 @@ __device__ __forceinline__ void side_rev(const SideFwd &s, double g, const doubl
     aP[P_BZ] += a_B[2];
 }
 
+// a side chosen at compile time (left = true)
+template <bool LEFT>
+struct SideTag {
+    static constexpr bool value = LEFT;
+};
+
+// what the face solvers read of a side after side_fwd: its conserved
+// state, flux and characteristic speeds (18 words instead of SideFwd's 60,
+// so that the face's reverse does not hold both sides' intermediates)
+struct SideOut {
+    double u[NCONS], f[NCONS], cp, cm;
+};
+
+template <int IDIR>
+__device__ __forceinline__ void side_out(const double *P, double g, SideOut &o) {
+    SideFwd s;
+    side_fwd<IDIR>(P, g, s);
+    for (int k = 0; k < NCONS; ++k) {
+        o.u[k] = s.u[k];
+        o.f[k] = s.f[k];
+    }
+    o.cp = s.cp;
+    o.cm = s.cm;
+}
+
+// a copy the optimiser cannot see through, so that a recomputation from it
+// is not merged with the earlier evaluation (whose intermediates would then
+// stay live in between)
+__device__ __forceinline__ double opaque(double x) {
+#ifdef __CUDA_ARCH__
+    asm volatile("mov.b64 %0, %0;" : "+d"(x));
+#endif
+    return x;
+}
+
+// side_rev with the side's intermediates recomputed from its primitives
+template <int IDIR>
+__device__ __forceinline__ void side_rev_from(const double *P, double g, const double *au,
+                                              const double *af, double acp, double acm,
+                                              double *aP) {
+    double Pc[NPRIM];
+    for (int k = 0; k < NPRIM; ++k) Pc[k] = opaque(P[k]);
+    SideFwd s;
+    side_fwd<IDIR>(Pc, g, s);
+    side_rev<IDIR>(s, g, au, af, acp, acm, aP);
+}
+
 // srmhd_fluxes' wave speeds: adjoints of cmax / cmin -> the sides' cp / cm
 struct Speeds {
     double cmax, cmin;
     bool small;
 };
 
-__device__ __forceinline__ Speeds speeds(const SideFwd &L, const SideFwd &R) {
+__device__ __forceinline__ Speeds speeds(const SideOut &L, const SideOut &R) {
     Speeds s;
     s.cmax = clamp_lo(tmax(L.cp, R.cp), 0.0);
     s.cmin = clamp_lo(tmax(-L.cm, -R.cm), 0.0);
@@ -259,7 +306,7 @@ __device__ __forceinline__ Speeds speeds(const SideFwd &L, const SideFwd &R) {
     return s;
 }
 
-__device__ __forceinline__ void speeds_rev(const SideFwd &L, const SideFwd &R, const Speeds &s,
+__device__ __forceinline__ void speeds_rev(const SideOut &L, const SideOut &R, const Speeds &s,
                                            double acmax, double acmin, double &acpL,
                                            double &acpR, double &acmL, double &acmR) {
     acpL = acpR = acmL = acmR = 0.0;
@@ -303,9 +350,9 @@ __device__ __forceinline__ void hu_rev(double fL, double fR, double uL, double u
 template <int IDIR>
 __device__ __forceinline__ void hlle_face_vjp(const double *PL, const double *PR, double gamma,
                                               const double *aF, double *aPL, double *aPR) {
-    SideFwd L, R;
-    side_fwd<IDIR>(PL, gamma, L);
-    side_fwd<IDIR>(PR, gamma, R);
+    SideOut L, R;
+    side_out<IDIR>(PL, gamma, L);
+    side_out<IDIR>(PR, gamma, R);
     const Speeds sp = speeds(L, R);
     const double cm = sp.cmin, cx = sp.cmax;
     double auL[NCONS] = {}, afL[NCONS] = {}, auR[NCONS] = {}, afR[NCONS] = {};
@@ -318,8 +365,8 @@ __device__ __forceinline__ void hlle_face_vjp(const double *PL, const double *PR
     }
     double acpL, acpR, acmL, acmR;
     speeds_rev(L, R, sp, acx, acm, acpL, acpR, acmL, acmR);
-    side_rev<IDIR>(L, gamma, auL, afL, acpL, acmL, aPL);
-    side_rev<IDIR>(R, gamma, auR, afR, acpR, acmR, aPR);
+    side_rev_from<IDIR>(PL, gamma, auL, afL, acpL, acmL, aPL);
+    side_rev_from<IDIR>(PR, gamma, auR, afR, acpR, acmR, aPR);
 }
 
 // ── HLLD (hlld.py:366-605, :1202-1543) at a solved p* ─────────────────────
@@ -354,6 +401,21 @@ struct VarsFwd {
 
 __device__ __forceinline__ void vars_fwd(const double *c, double SL, double SR, double p,
                                          VarsFwd &v) {
+    // The quantities the forward solver itself produces are taken from its
+    // own hlld_vars, so that they are bit-identical to the values the forward
+    // step saw (its fast forms multiply by a shared reciprocal where this
+    // restatement divides, a one-rounding difference that would move the
+    // tiny-denominator decisions: KaL == KaR exactly at a degenerate contact
+    // in the forward but not here).  The intermediates between them, which
+    // only the reverse needs, are recomputed.
+    HlldR<double> C;
+    C.RSiL = c[R_SiL]; C.RSiR = c[R_SiR]; C.RS1L = c[R_S1L]; C.RS1R = c[R_S1R];
+    C.RS2L = c[R_S2L]; C.RS2R = c[R_S2R]; C.RBiL = c[R_BiL]; C.RBiR = c[R_BiR];
+    C.RB1L = c[R_B1L]; C.RB1R = c[R_B1R]; C.RB2L = c[R_B2L]; C.RB2R = c[R_B2R];
+    C.RTL = c[R_TL]; C.RTR = c[R_TR]; C.RDL = c[R_DL]; C.RDR = c[R_DR];
+    C.S_L = SL; C.S_R = SR; C.BnL = c[R_BnL]; C.BnR = c[R_BnR]; C.cm = c[R_cm]; C.cx = c[R_cx];
+    HlldV<double> h;
+    hlld_vars<true>(C, p, h);
     const double cm = c[R_cm], cx = c[R_cx], ncm = -cm;
     const double BnL = c[R_BnL], BnR = c[R_BnR];
     v.AL = c[R_SiL] - ncm * c[R_TL] + p * (1.0 - cm * cm);
@@ -370,61 +432,60 @@ __device__ __forceinline__ void vars_fwd(const double *c, double SL, double SR, 
     v.dXR = safe_den(v.XR);
     v.nvaL = BnL * (v.AL * BnL + ncm * v.CL) - (v.AL + v.GL) * (p + c[R_SiL]);
     v.nvaR = BnR * (v.AR * BnR + cx * v.CR) - (v.AR + v.GR) * (p + c[R_SiR]);
-    v.vaL = v.nvaL / v.dXL;
-    v.vaR = v.nvaR / v.dXR;
+    v.vaL = h.vaL;
+    v.vaR = h.vaR;
     v.n1L = v.CL + BnL * (ncm * c[R_SiL] - c[R_TL]);
     v.n1R = v.CR + BnR * (cx * c[R_SiR] - c[R_TR]);
-    v.vt1aL = (v.QL * c[R_S1L] + c[R_B1L] * v.n1L) / v.dXL;
-    v.vt1aR = (v.QR * c[R_S1R] + c[R_B1R] * v.n1R) / v.dXR;
-    v.vt2aL = (v.QL * c[R_S2L] + c[R_B2L] * v.n1L) / v.dXL;
-    v.vt2aR = (v.QR * c[R_S2R] + c[R_B2R] * v.n1R) / v.dXR;
+    v.vt1aL = h.vt1aL;
+    v.vt1aR = h.vt1aR;
+    v.vt2aL = h.vt2aL;
+    v.vt2aR = h.vt2aR;
     v.dAL = ncm - v.vaL;
     v.dAR = cx - v.vaR;
     v.sAL = safe_den(v.dAL);
     v.sAR = safe_den(v.dAR);
-    v.Bt1aL = (c[R_B1L] - BnL * v.vt1aL) / v.sAL;
-    v.Bt1aR = (c[R_B1R] - BnR * v.vt1aR) / v.sAR;
-    v.Bt2aL = (c[R_B2L] - BnL * v.vt2aL) / v.sAL;
-    v.Bt2aR = (c[R_B2R] - BnR * v.vt2aR) / v.sAR;
+    v.Bt1aL = h.Bt1aL;
+    v.Bt1aR = h.Bt1aR;
+    v.Bt2aL = h.Bt2aL;
+    v.Bt2aR = h.Bt2aR;
     v.vRSL = v.vaL * c[R_SiL] + v.vt1aL * c[R_S1L] + v.vt2aL * c[R_S2L];
     v.vRSR = v.vaR * c[R_SiR] + v.vt1aR * c[R_S1R] + v.vt2aR * c[R_S2R];
     v.waL = p + (c[R_TL] - v.vRSL) / v.sAL;
     v.waR = p + (c[R_TR] - v.vRSR) / v.sAR;
-    v.sqL = sqrt(clamp_lo(v.waL, 0.0));
-    v.sqR = sqrt(clamp_lo(v.waR, 0.0));
+    v.sqL = h.sqL;
+    v.sqR = h.sqR;
     v.dL = ncm * p + c[R_TL] - BnL * SL * v.sqL;
     v.dR = cx * p + c[R_TR] + BnR * SR * v.sqR;
     v.sdL = safe_den(v.dL);
     v.sdR = safe_den(v.dR);
-    v.KaL = (c[R_SiL] + p - c[R_BiL] * SL * v.sqL) / v.sdL;
-    v.KaR = (c[R_SiR] + p + c[R_BiR] * SR * v.sqR) / v.sdR;
-    v.Kt1aL = (c[R_S1L] - c[R_B1L] * SL * v.sqL) / v.sdL;
-    v.Kt1aR = (c[R_S1R] + c[R_B1R] * SR * v.sqR) / v.sdR;
-    v.Kt2aL = (c[R_S2L] - c[R_B2L] * SL * v.sqL) / v.sdL;
-    v.Kt2aR = (c[R_S2R] + c[R_B2R] * SR * v.sqR) / v.sdR;
+    v.KaL = h.laL;
+    v.KaR = h.laR;
+    v.Kt1aL = h.Kt1aL;
+    v.Kt1aR = h.Kt1aR;
+    v.Kt2aL = h.Kt2aL;
+    v.Kt2aR = h.Kt2aR;
     v.dll = v.KaR - v.KaL;
     v.sdll = safe_den(v.dll);
     v.nB1 = (v.Bt1aR * (v.KaR - v.vaR) + BnR * v.vt1aR) - (v.Bt1aL * (v.KaL - v.vaL) + BnL * v.vt1aL);
     v.nB2 = (v.Bt2aR * (v.KaR - v.vaR) + BnR * v.vt2aR) - (v.Bt2aL * (v.KaL - v.vaL) + BnL * v.vt2aL);
-    v.Bt1c = v.nB1 / v.sdll;
-    v.Bt2c = v.nB2 / v.sdll;
-    v.KaL2 = v.KaL * v.KaL + v.Kt1aL * v.Kt1aL + v.Kt2aL * v.Kt2aL;
-    v.KaR2 = v.KaR * v.KaR + v.Kt1aR * v.Kt1aR + v.Kt2aR * v.Kt2aR;
-    v.KaLBc = v.KaL * BnR + v.Kt1aL * v.Bt1c + v.Kt2aL * v.Bt2c;
-    v.KaRBc = v.KaR * BnR + v.Kt1aR * v.Bt1c + v.Kt2aR * v.Bt2c;
-    v.DaL = c[R_DL] / v.sAL;
-    v.DaR = c[R_DR] / v.sAR;
+    v.Bt1c = h.Bt1c;
+    v.Bt2c = h.Bt2c;
+    v.KaL2 = h.KaL2;
+    v.KaR2 = h.KaR2;
+    v.KaLBc = h.KaLBc;
+    v.KaRBc = h.KaRBc;
+    v.DaL = h.DaL;
+    v.DaR = h.DaR;
     v.vBaL = v.vaL * BnL + v.vt1aL * v.Bt1aL + v.vt2aL * v.Bt2aL;
     v.vBaR = v.vaR * BnR + v.vt1aR * v.Bt1aR + v.vt2aR * v.Bt2aR;
-    v.TauaL = (c[R_TL] + p * v.vaL - v.vBaL * BnL) / v.sAL - v.DaL;
-    v.TauaR = (c[R_TR] + p * v.vaR - v.vBaR * BnR) / v.sAR - v.DaR;
-    const double eL = v.TauaL + v.DaL + p, eR = v.TauaR + v.DaR + p;
-    v.SaL = eL * v.vaL - v.vBaL * BnL;
-    v.SaR = eR * v.vaR - v.vBaR * BnR;
-    v.St1aL = eL * v.vt1aL - v.vBaL * v.Bt1aL;
-    v.St1aR = eR * v.vt1aR - v.vBaR * v.Bt1aR;
-    v.St2aL = eL * v.vt2aL - v.vBaL * v.Bt2aL;
-    v.St2aR = eR * v.vt2aR - v.vBaR * v.Bt2aR;
+    v.TauaL = h.TauaL;
+    v.TauaR = h.TauaR;
+    v.SaL = h.SaL;
+    v.SaR = h.SaR;
+    v.St1aL = h.St1aL;
+    v.St1aR = h.St1aR;
+    v.St2aL = h.St2aL;
+    v.St2aR = h.St2aR;
 }
 
 // adjoints of VarsFwd's outputs (only the fields the assembly and the
@@ -661,9 +722,9 @@ __device__ __forceinline__ void hlld_face_vjp(const double *PL, const double *PR
                                               double p_star, bool failed, const double *aF,
                                               double *aPL, double *aPR) {
     constexpr int i = IDIR, t1 = (IDIR + 1) % 3, t2 = (IDIR + 2) % 3;
-    SideFwd L, R;
-    side_fwd<IDIR>(PL, gamma, L);
-    side_fwd<IDIR>(PR, gamma, R);
+    SideOut L, R;
+    side_out<IDIR>(PL, gamma, L);
+    side_out<IDIR>(PR, gamma, R);
     const Speeds sp = speeds(L, R);
     const double cm = sp.cmin, cx = sp.cmax;
     double auL[NCONS] = {}, afL[NCONS] = {}, auR[NCONS] = {}, afR[NCONS] = {};
@@ -740,101 +801,112 @@ __device__ __forceinline__ void hlld_face_vjp(const double *PL, const double *PR
         } else if (reg == 5) {
             for (int k = 0; k < NCONS; ++k) afR[k] += aF[k];
         } else if (reg == 1 || reg == 4) {
-            // fa = f + (-cm)(ua - u) on the left, f + cx (ua - u) on the right
-            const bool left = reg == 1;
-            const SideFwd &S = left ? L : R;
-            const double sp_ = left ? -cm : cx;
-            for (int k = 0; k < NCONS; ++k) {
-                const double g = aF[k];
-                if (left) { afL[k] += g; a_uaL[k] += g * sp_; auL[k] -= g * sp_; acm -= g * (uaL[k] - S.u[k]); }
-                else { afR[k] += g; a_uaR[k] += g * sp_; auR[k] -= g * sp_; acx += g * (uaR[k] - S.u[k]); }
-            }
-        } else {
-            // contact regions: f = fa + la (uc - ua)
-            const bool left = reg == 2;
-            const SideFwd &S = left ? L : R;
-            const double sp_ = left ? -cm : cx;
-            const double la = left ? laL : laR;
-            const double va = left ? V.vaL : V.vaR;
-            const double *ua = left ? uaL : uaR;
-            double *a_ua = left ? a_uaL : a_uaR;
-            const double faT = S.f[C_TAU] + sp_ * (ua[C_TAU] - S.u[C_TAU]);
-            const double dn = la - vc;
-            const double sdn = safe_den(dn);
-            const double rD = (la - va) / sdn;
-            const double ucD = ua[C_D] * rD;
-            const double nT = la * ua[C_TAU] - faT + p * vc - vBc * Bc[i];
-            const double ucT = nT / sdn;
-            double uc[NCONS];
-            for (int k = 0; k < NCONS; ++k) {
-                if (k == C_D) uc[k] = ucD;
-                else if (k == C_TAU) uc[k] = ucT;
-                else if (k >= C_BX) uc[k] = Bc[k - C_BX];
-                else uc[k] = (ucT + p + ucD) * vcomp[k - C_SX] - vBc * Bc[k - C_SX];
-            }
-            double a_la = 0, a_ucD = 0, a_ucT = 0, a_uc[NCONS] = {}, a_sp = 0;
-            double a_vcomp[3] = {0, 0, 0}, a_Bc[3] = {0, 0, 0};
-            for (int k = 0; k < NCONS; ++k) {
-                const double g = aF[k];
-                const double fa = S.f[k] + sp_ * (ua[k] - S.u[k]);
-                (void)fa;
-                // f = fa + la (uc - ua), fa = fS + sp (ua - uS)
-                if (left) afL[k] += g; else afR[k] += g;
-                a_sp += g * (ua[k] - S.u[k]);
-                a_ua[k] += g * sp_ - g * la;
-                if (left) auL[k] -= g * sp_; else auR[k] -= g * sp_;
-                a_la += g * (uc[k] - ua[k]);
-                a_uc[k] += g * la;
-            }
-            // uc components
-            for (int k = 0; k < NCONS; ++k) {
-                const double g = a_uc[k];
-                if (k == C_D) a_ucD += g;
-                else if (k == C_TAU) a_ucT += g;
-                else if (k >= C_BX) a_Bc[k - C_BX] += g;
-                else {
-                    const int cc = k - C_SX;
-                    a_ucT += g * vcomp[cc];
-                    ap += g * vcomp[cc];
-                    a_ucD += g * vcomp[cc];
-                    a_vcomp[cc] += g * (ucT + p + ucD);
-                    a_vBc -= g * Bc[cc];
-                    a_Bc[cc] -= g * vBc;
+            // the side is a template argument, so that every selection below
+            // is resolved at compile time (a runtime choice between the two
+            // sides' arrays would put them in local memory)
+            auto outer_star = [&](auto side) {
+                // fa = f + (-cm)(ua - u) on the left, f + cx (ua - u) on the right
+                constexpr bool left = decltype(side)::value;
+                const SideOut &S = left ? L : R;
+                const double sp_ = left ? -cm : cx;
+                for (int k = 0; k < NCONS; ++k) {
+                    const double g = aF[k];
+                    if (left) { afL[k] += g; a_uaL[k] += g * sp_; auL[k] -= g * sp_; acm -= g * (uaL[k] - S.u[k]); }
+                    else { afR[k] += g; a_uaR[k] += g * sp_; auR[k] -= g * sp_; acx += g * (uaR[k] - S.u[k]); }
                 }
-            }
-            // ucT = nT / sdn, nT = la uaT - faT + p vc - vBc Bc_i
-            double a_nT = 0, a_dn = 0;
-            div_rev(a_ucT, ucT, sdn, dn, a_nT, a_dn);
-            a_la += a_nT * ua[C_TAU];
-            a_ua[C_TAU] += a_nT * la;
-            const double a_faT = -a_nT;
-            ap += a_nT * vc;
-            a_vc += a_nT * p;
-            a_vBc -= a_nT * Bc[i];
-            a_Bc[i] -= a_nT * vBc;
-            // faT = fS_tau + sp (ua_tau - uS_tau)
-            if (left) afL[C_TAU] += a_faT; else afR[C_TAU] += a_faT;
-            a_sp += a_faT * (ua[C_TAU] - S.u[C_TAU]);
-            a_ua[C_TAU] += a_faT * sp_;
-            if (left) auL[C_TAU] -= a_faT * sp_; else auR[C_TAU] -= a_faT * sp_;
-            // ucD = ua_D rD, rD = (la - va) / sdn
-            a_ua[C_D] += a_ucD * rD;
-            const double a_rD = a_ucD * ua[C_D];
-            double a_nrD = 0;
-            div_rev(a_rD, rD, sdn, dn, a_nrD, a_dn);
-            a_la += a_nrD;
-            if (left) a.vaL -= a_nrD; else a.vaR -= a_nrD;
-            // dn = la - vc
-            a_la += a_dn;
-            a_vc -= a_dn;
-            if (left) { a.KaL += a_la; acm -= a_sp; }
-            else { a.KaR += a_la; acx += a_sp; }
-            a_vc += a_vcomp[i];
-            a_vt1 += a_vcomp[t1];
-            a_vt2 += a_vcomp[t2];
-            a_BnRc += a_Bc[i];
-            a_Bt1c += a_Bc[t1];
-            a_Bt2c += a_Bc[t2];
+            };
+            if (reg == 1) outer_star(SideTag<true>{});
+            else outer_star(SideTag<false>{});
+        } else {
+            auto contact = [&](auto side) {
+                // contact regions: f = fa + la (uc - ua)
+                constexpr bool left = decltype(side)::value;
+                const SideOut &S = left ? L : R;
+                const double sp_ = left ? -cm : cx;
+                const double la = left ? laL : laR;
+                const double va = left ? V.vaL : V.vaR;
+                const double *ua = left ? uaL : uaR;
+                double *a_ua = left ? a_uaL : a_uaR;
+                const double faT = S.f[C_TAU] + sp_ * (ua[C_TAU] - S.u[C_TAU]);
+                const double dn = la - vc;
+                const double sdn = safe_den(dn);
+                const double rD = (la - va) / sdn;
+                const double ucD = ua[C_D] * rD;
+                const double nT = la * ua[C_TAU] - faT + p * vc - vBc * Bc[i];
+                const double ucT = nT / sdn;
+                double uc[NCONS];
+                for (int k = 0; k < NCONS; ++k) {
+                    if (k == C_D) uc[k] = ucD;
+                    else if (k == C_TAU) uc[k] = ucT;
+                    else if (k >= C_BX) uc[k] = Bc[k - C_BX];
+                    else uc[k] = (ucT + p + ucD) * vcomp[k - C_SX] - vBc * Bc[k - C_SX];
+                }
+                double a_la = 0, a_ucD = 0, a_ucT = 0, a_uc[NCONS] = {}, a_sp = 0;
+                double a_vcomp[3] = {0, 0, 0}, a_Bc[3] = {0, 0, 0};
+                for (int k = 0; k < NCONS; ++k) {
+                    const double g = aF[k];
+                    const double fa = S.f[k] + sp_ * (ua[k] - S.u[k]);
+                    (void)fa;
+                    // f = fa + la (uc - ua), fa = fS + sp (ua - uS)
+                    if (left) afL[k] += g; else afR[k] += g;
+                    a_sp += g * (ua[k] - S.u[k]);
+                    a_ua[k] += g * sp_ - g * la;
+                    if (left) auL[k] -= g * sp_; else auR[k] -= g * sp_;
+                    a_la += g * (uc[k] - ua[k]);
+                    a_uc[k] += g * la;
+                }
+                // uc components
+                for (int k = 0; k < NCONS; ++k) {
+                    const double g = a_uc[k];
+                    if (k == C_D) a_ucD += g;
+                    else if (k == C_TAU) a_ucT += g;
+                    else if (k >= C_BX) a_Bc[k - C_BX] += g;
+                    else {
+                        const int cc = k - C_SX;
+                        a_ucT += g * vcomp[cc];
+                        ap += g * vcomp[cc];
+                        a_ucD += g * vcomp[cc];
+                        a_vcomp[cc] += g * (ucT + p + ucD);
+                        a_vBc -= g * Bc[cc];
+                        a_Bc[cc] -= g * vBc;
+                    }
+                }
+                // ucT = nT / sdn, nT = la uaT - faT + p vc - vBc Bc_i
+                double a_nT = 0, a_dn = 0;
+                div_rev(a_ucT, ucT, sdn, dn, a_nT, a_dn);
+                a_la += a_nT * ua[C_TAU];
+                a_ua[C_TAU] += a_nT * la;
+                const double a_faT = -a_nT;
+                ap += a_nT * vc;
+                a_vc += a_nT * p;
+                a_vBc -= a_nT * Bc[i];
+                a_Bc[i] -= a_nT * vBc;
+                // faT = fS_tau + sp (ua_tau - uS_tau)
+                if (left) afL[C_TAU] += a_faT; else afR[C_TAU] += a_faT;
+                a_sp += a_faT * (ua[C_TAU] - S.u[C_TAU]);
+                a_ua[C_TAU] += a_faT * sp_;
+                if (left) auL[C_TAU] -= a_faT * sp_; else auR[C_TAU] -= a_faT * sp_;
+                // ucD = ua_D rD, rD = (la - va) / sdn
+                a_ua[C_D] += a_ucD * rD;
+                const double a_rD = a_ucD * ua[C_D];
+                double a_nrD = 0;
+                div_rev(a_rD, rD, sdn, dn, a_nrD, a_dn);
+                a_la += a_nrD;
+                if (left) a.vaL -= a_nrD; else a.vaR -= a_nrD;
+                // dn = la - vc
+                a_la += a_dn;
+                a_vc -= a_dn;
+                if (left) { a.KaL += a_la; acm -= a_sp; }
+                else { a.KaR += a_la; acx += a_sp; }
+                a_vc += a_vcomp[i];
+                a_vt1 += a_vcomp[t1];
+                a_vt2 += a_vcomp[t2];
+                a_BnRc += a_Bc[i];
+                a_Bt1c += a_Bc[t1];
+                a_Bt2c += a_Bc[t2];
+            };
+            if (reg == 2) contact(SideTag<true>{});
+            else contact(SideTag<false>{});
         }
         // ua arrays -> V fields and Bn
         ac[R_BnL] += a_uaL[C_BX + i];
@@ -905,8 +977,8 @@ __device__ __forceinline__ void hlld_face_vjp(const double *PL, const double *PR
     }
     double acpL, acpR, acmL, acmR;
     speeds_rev(L, R, sp, acx, acm, acpL, acpR, acmL, acmR);
-    side_rev<IDIR>(L, gamma, auL, afL, acpL, acmL, aPL);
-    side_rev<IDIR>(R, gamma, auR, afR, acpR, acmR, aPR);
+    side_rev_from<IDIR>(PL, gamma, auL, afL, acpL, acmL, aPL);
+    side_rev_from<IDIR>(PR, gamma, auR, afR, acpR, acmR, aPR);
 }
 
 }  // namespace vjp
