@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import datetime
 import json
 import os
 import statistics
@@ -58,8 +59,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint/forward cost of the 512^2 rotor gradient study")
-    ap.add_argument("--workload", default="rotor", choices=["rotor", "tubes"],
-                    help="rotor: the 2D rotor step (default); tubes: the batched-tube launch")
+    ap.add_argument("--workload", default="rotor", choices=["rotor", "tubes", "adjoint"],
+                    help="rotor: the 2D rotor step (default); tubes: the batched-tube launch; "
+                         "adjoint: the rotor gradient study alone (adjoint/forward cost)")
+    ap.add_argument("--adjoint-n", type=int, default=512)
+    ap.add_argument("--adjoint-steps", type=int, default=200)
+    ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint interval")
     ap.add_argument("--tubes", type=int, default=4096)
     ap.add_argument("--chunk", type=float, default=0.01,
                     help="tubes: simulated time every tube advances per step")
@@ -337,7 +342,7 @@ def run_ours(a):
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", device_id=dev,
-                                timeout=__import__("datetime").timedelta(seconds=300))
+                                timeout=datetime.timedelta(seconds=300))
 
     main = _timed_rotor(a, a.precision, dev, world, record=True)
     g, st, stepper = main["g"], main["st"], main["stepper"]
@@ -418,9 +423,9 @@ def run_ours(a):
         from hlld_ai_b200.adjoint import RotorCase, rotor_gradients
 
         torch.cuda.empty_cache()
-        r = rotor_gradients(RotorCase(n=512, steps=200, checkpoint_every=20), device=dev)
-        adj = {"workload": "rotor 512^2, FP64 HLLD + PLM(MC) + CT, 200 SSP-RK3 steps, "
-                           "checkpoint every 20, J = sum w |B_c|^2 / 2",
+        r = rotor_gradients(RotorCase(n=a.adjoint_n, steps=a.adjoint_steps,
+                                      checkpoint_every=a.adjoint_every), device=dev)
+        adj = {"workload": _adjoint_workload(a),
                "forward_ms": r["forward_ms"], "adjoint_ms": r["adjoint_ms"],
                "adjoint_over_forward": r["adjoint_ms"] / r["forward_ms"],
                "J": r["J"], "dJ_domega": r["grad_omega"]}
@@ -509,7 +514,7 @@ def run_tubes(a):
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", device_id=dev,
-                                timeout=__import__("datetime").timedelta(seconds=300))
+                                timeout=datetime.timedelta(seconds=300))
     # tubes are independent units: each rank runs its own seeded batch
     states = random_tubes(a.tubes, seed=20261203 + rank)
     precision = "mixed" if a.precision == "mixed" else a.precision
@@ -623,12 +628,55 @@ def run_tubes(a):
     return 0
 
 
+def _adjoint_workload(a):
+    return (f"rotor {a.adjoint_n}^2, FP64 HLLD + PLM(MC) + CT, {a.adjoint_steps} SSP-RK3 steps, "
+            f"checkpoint every {a.adjoint_every}, J = sum w |B_c|^2 / 2")
+
+
+def run_adjoint(a):
+    """The rotor gradient study alone: J and dJ/d(rho0, omega) by the
+    checkpointed discrete adjoint; the line reports the median over --steps
+    runs of the adjoint's time over the forward run's (both timed with CUDA
+    events inside rotor_gradients).
+    Replicas under torchrun; rank 0 prints."""
+    import torch
+    import torch.distributed as dist
+    from hlld_ai_b200.adjoint import RotorCase, rotor_gradients
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    case = RotorCase(n=a.adjoint_n, steps=a.adjoint_steps, checkpoint_every=a.adjoint_every)
+    runs = [rotor_gradients(case, device=dev) for _ in range(max(1, a.steps))]
+    ratios = [r["adjoint_ms"] / r["forward_ms"] for r in runs]
+    if world > 1:
+        m = torch.tensor([max(ratios)], dtype=torch.float64, device=dev)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": "adjoint time / forward time", "value": statistics.median(ratios),
+                "unit": "x",
+                "n_gpus": world, "steps": len(runs), "warmup": 0, "higher_is_better": False,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": _adjoint_workload(a)},
+                "runs": [{"forward_ms": r["forward_ms"], "adjoint_ms": r["adjoint_ms"]} for r in runs],
+                "J": runs[0]["J"], "dJ_domega": runs[0]["grad_omega"]}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
     if a.workload == "tubes":
         return run_tubes(a)
+    if a.workload == "adjoint":
+        return run_adjoint(a)
     return run_ours(a)
 
 

@@ -286,9 +286,10 @@ def rotor_gradients(case: RotorCase, device="cuda"):
         dt = float(run.stepper.compute_dt(s, case.cfl).item())
         dts.append(dt)
         run.stepper.step(s, dt, "rk3")
-    # warm-up: two steps forward and back load the kernels and fill the
-    # allocator's pools, so the timed run measures the steady state
-    run.forward(s0, dts[:2])
+    # warm-up: one whole checkpoint segment forward and back loads the
+    # kernels and grows the allocator's pools to the segment's states, so the
+    # timed run measures the steady state
+    run.forward(s0, dts[:min(case.checkpoint_every, case.steps)])
     run.backward(_zeros_state(grid, run.device))
     torch.cuda.synchronize()
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))

@@ -32,6 +32,12 @@
 namespace hlld {
 namespace HLLD_NS {
 
+// blocks of kThreads per SM the adjoint sweep is compiled for (its register
+// cap: 65536 / (kThreads * min blocks), at most 255)
+#ifndef HLLD_ADJ_SWEEP_MIN_BLOCKS
+#define HLLD_ADJ_SWEEP_MIN_BLOCKS 2
+#endif
+
 constexpr int kAdjDirs = 15;  // rho, p, vx, vy, vz, B_t, Bz per side + B_n
 constexpr int kMaxNW = 8;     // widest reconstruction window (MP7)
 
@@ -48,7 +54,7 @@ struct AdjSweepParams {
 
 // Adjoint of one face of sweep_kernel<AXIS, LIM, SOLVER> (FP64).
 template <int AXIS, int LIM, int SOLVER>
-__global__ void __launch_bounds__(kThreads) adj_sweep_kernel(const AdjSweepParams p) {
+__global__ void __launch_bounds__(kThreads, HLLD_ADJ_SWEEP_MIN_BLOCKS) adj_sweep_kernel(const AdjSweepParams p) {
     constexpr int S = Stencil<LIM>::S;
     constexpr int NW = 2 * S + 2;
     const Grid &g = p.g;

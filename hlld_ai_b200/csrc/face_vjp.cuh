@@ -40,16 +40,18 @@ __device__ __forceinline__ void side_fwd(const double *P, double g, SideFwd &s) 
     s.v2s = clamp_hi(s.v2, 1.0 - 1e-10);
     s.W = 1.0 / sqrt(1.0 - s.v2s);
     const double W = s.W;
+    // (the intermediates of the reverse only: shared reciprocals)
+    const double iW = 1.0 / W, irho = 1.0 / rho;
     s.e = tmax(eps, 0.0);
     s.press = 0.0 + (s.e - 0.0) * rho * (g - 1.0);
-    s.he = 1.0 + eps + s.press / rho;
-    s.cs2 = (g * 0.0 + g * (s.press - 0.0)) / (rho * s.he);
+    s.he = 1.0 + eps + s.press * irho;
+    s.cs2 = (g * 0.0 + g * (s.press - 0.0)) * irho / s.he;
     s.B2 = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
     s.vdotB = v[0] * B[0] + v[1] * B[1] + v[2] * B[2];
-    s.b2 = s.B2 / (W * W) + s.vdotB * s.vdotB;
+    s.b2 = s.B2 * (iW * iW) + s.vdotB * s.vdotB;
     s.bt = W * s.vdotB;
-    for (int i = 0; i < 3; ++i) s.bs[i] = B[i] / W + s.vdotB * v[i] * W;
-    s.h = 1.0 + eps + s.press / rho;
+    for (int i = 0; i < 3; ++i) s.bs[i] = B[i] * iW + s.vdotB * v[i] * W;
+    s.h = 1.0 + eps + s.press * irho;
     s.Y = rho * s.h + s.b2;
     s.X = s.b2 / s.Y;
     s.v02 = s.cs2 + s.X * (1.0 - s.cs2);
@@ -63,8 +65,9 @@ __device__ __forceinline__ void side_fwd(const double *P, double g, SideFwd &s) 
     s.disc = s.b * s.b - 4.0 * s.a * s.c;
     s.det = sqrt(clamp_lo(s.disc, 0.0));
     s.as = clamp_lo(s.a, K<double>::tiny);
-    s.c1 = 0.5 * (s.det - s.b) / s.as;
-    s.c2 = -0.5 * (s.det + s.b) / s.as;
+    const double ias = 1.0 / s.as;
+    s.c1 = 0.5 * (s.det - s.b) * ias;
+    s.c2 = -0.5 * (s.det + s.b) * ias;
     s.cp = tmax(s.c1, s.c2);
     s.cm = tmin(s.c1, s.c2);
     s.d = rho * W;
@@ -95,6 +98,8 @@ __device__ __forceinline__ void side_rev(const SideFwd &s, double g, const doubl
     const double rho = P[P_RHO], eps = P[P_EPS];
     const double v[3] = {P[P_VX], P[P_VY], P[P_VZ]}, B[3] = {P[P_BX], P[P_BY], P[P_BZ]};
     const double W = s.W, vd = v[IDIR], bdir = s.bs[IDIR];
+    // reciprocals of the shared denominators
+    const double ias = 1.0 / s.as, irho = 1.0 / rho, iW = 1.0 / W, iY = 1.0 / s.Y;
     double a_v[3] = {0, 0, 0}, a_B[3] = {0, 0, 0}, a_bs[3] = {0, 0, 0};
     double a_W = 0, a_rho = 0, a_eps = 0, a_vd = 0, a_bdir = 0, a_d = 0, a_rhb2 = 0, a_W2 = 0;
     double a_Pb2 = 0, a_bt = 0, a_press = 0, a_b2 = 0, a_h = 0, a_vdotB = 0, a_B2 = 0;
@@ -164,12 +169,12 @@ __device__ __forceinline__ void side_rev(const SideFwd &s, double g, const doubl
         if (s.c1 < s.c2) a_c2 += acp; else a_c1 += acp;
         if (s.c2 < s.c1) a_c2 += acm; else a_c1 += acm;
         double a_det = 0, a_b = 0, a_as = 0, a_a = 0, a_c = 0, a_u0sq = 0, a_omv = 0, a_v02 = 0;
-        a_det += a_c1 * 0.5 / s.as;
-        a_b -= a_c1 * 0.5 / s.as;
-        a_as -= a_c1 * s.c1 / s.as;
-        a_det -= a_c2 * 0.5 / s.as;
-        a_b -= a_c2 * 0.5 / s.as;
-        a_as -= a_c2 * s.c2 / s.as;
+        a_det += a_c1 * 0.5 * ias;
+        a_b -= a_c1 * 0.5 * ias;
+        a_as -= a_c1 * s.c1 * ias;
+        a_det -= a_c2 * 0.5 * ias;
+        a_b -= a_c2 * 0.5 * ias;
+        a_as -= a_c2 * s.c2 * ias;
         if (!(s.a < K<double>::tiny)) a_a += a_as;
         const double a_dc = s.det > 0.0 ? a_det * 0.5 / s.det : 0.0;
         const double a_disc = s.disc < 0.0 ? 0.0 : a_dc;
@@ -191,34 +196,34 @@ __device__ __forceinline__ void side_rev(const SideFwd &s, double g, const doubl
         // v02 = cs2 + X (1 - cs2), X = b2 / Y, Y = rho h + b2
         double a_cs2 = a_v02 * (1.0 - s.X);
         const double a_X = a_v02 * (1.0 - s.cs2);
-        a_b2 += a_X / s.Y;
-        const double a_Y = -a_X * s.X / s.Y;
+        a_b2 += a_X * iY;
+        const double a_Y = -a_X * s.X * iY;
         a_rho += a_Y * s.h;
         a_h += a_Y * rho;
         a_b2 += a_Y;
         // cs2 = g press / (rho he), he = 1 + eps + press / rho
-        a_press += a_cs2 * g / (rho * s.he);
-        a_rho -= a_cs2 * s.cs2 / rho;
+        a_press += a_cs2 * g * irho / s.he;
+        a_rho -= a_cs2 * s.cs2 * irho;
         const double a_he = -a_cs2 * s.cs2 / s.he;
         a_eps += a_he;
-        a_press += a_he / rho;
-        a_rho -= a_he * s.press / (rho * rho);
+        a_press += a_he * irho;
+        a_rho -= a_he * s.press * irho * irho;
     }
     // h = 1 + eps + press / rho
     a_eps += a_h;
-    a_press += a_h / rho;
-    a_rho -= a_h * s.press / (rho * rho);
+    a_press += a_h * irho;
+    a_rho -= a_h * s.press * irho * irho;
     // bs, bt, b2
     for (int i = 0; i < 3; ++i) {
-        a_B[i] += a_bs[i] / W;
-        a_W += -a_bs[i] * B[i] / (W * W) + a_bs[i] * s.vdotB * v[i];
+        a_B[i] += a_bs[i] * iW;
+        a_W += -a_bs[i] * B[i] * iW * iW + a_bs[i] * s.vdotB * v[i];
         a_vdotB += a_bs[i] * v[i] * W;
         a_v[i] += a_bs[i] * s.vdotB * W;
     }
     a_W += a_bt * s.vdotB;
     a_vdotB += a_bt * W;
-    a_B2 += a_b2 / (W * W);
-    a_W -= a_b2 * 2.0 * s.B2 / (W * W * W);
+    a_B2 += a_b2 * iW * iW;
+    a_W -= a_b2 * 2.0 * s.B2 * iW * iW * iW;
     a_vdotB += 2.0 * a_b2 * s.vdotB;
     for (int i = 0; i < 3; ++i) {
         a_B[i] += 2.0 * a_B2 * B[i] + a_vdotB * v[i];
@@ -254,16 +259,17 @@ struct SideOut {
     double u[NCONS], f[NCONS], cp, cm;
 };
 
+// taken from the forward solver's own phys_side, so that u, f and the wave
+// speeds -- and through them every decision of the face -- are bit-identical
+// to the forward step's
 template <int IDIR>
 __device__ __forceinline__ void side_out(const double *P, double g, SideOut &o) {
-    SideFwd s;
-    side_fwd<IDIR>(P, g, s);
+    Side<double> s;
+    phys_side<IDIR, double>(P, g, s, o.cp, o.cm);
     for (int k = 0; k < NCONS; ++k) {
         o.u[k] = s.u[k];
         o.f[k] = s.f[k];
     }
-    o.cp = s.cp;
-    o.cm = s.cm;
 }
 
 // a copy the optimiser cannot see through, so that a recomputation from it
@@ -321,28 +327,21 @@ __device__ __forceinline__ void speeds_rev(const SideOut &L, const SideOut &R, c
     }
 }
 
-// hf / hu (hlld.py:161-168) in reverse: adjoints of fL, fR, uL, uR, cm, cx
+// hf (hlld.py:161-164) in reverse: adjoints of fL, fR, uL, uR, cm, cx.
+// (S = cx + cm is the same for every component; its reciprocal is one
+// common subexpression of the unrolled component loop.)
 __device__ __forceinline__ void hf_rev(double fL, double fR, double uL, double uR, double cm,
                                        double cx, double g, double &afL, double &afR,
                                        double &auL, double &auR, double &acm, double &acx) {
-    const double S = cx + cm, N = cx * fL + cm * fR - cx * cm * (uR - uL), q = N / S;
-    afL += g * cx / S;
-    afR += g * cm / S;
-    auR -= g * cx * cm / S;
-    auL += g * cx * cm / S;
-    acx += g * ((fL - cm * (uR - uL)) - q) / S;
-    acm += g * ((fR - cx * (uR - uL)) - q) / S;
-}
-__device__ __forceinline__ void hu_rev(double fL, double fR, double uL, double uR, double cm,
-                                       double cx, double g, double &afL, double &afR,
-                                       double &auL, double &auR, double &acm, double &acx) {
-    const double S = cx + cm, q = (cx * uR + cm * uL + fL - fR) / S;
-    auR += g * cx / S;
-    auL += g * cm / S;
-    afL += g / S;
-    afR -= g / S;
-    acx += g * (uR - q) / S;
-    acm += g * (uL - q) / S;
+    const double iS = 1.0 / (cx + cm);
+    const double N = cx * fL + cm * fR - cx * cm * (uR - uL), q = N * iS;
+    const double gi = g * iS;
+    afL += gi * cx;
+    afR += gi * cm;
+    auR -= gi * cx * cm;
+    auL += gi * cx * cm;
+    acx += gi * ((fL - cm * (uR - uL)) - q);
+    acm += gi * ((fR - cx * (uR - uL)) - q);
 }
 
 // ── HLLE (hlld.py:1005-1044) ──────────────────────────────────────────────
@@ -496,17 +495,22 @@ struct VarsAdj {
     double DaL, DaR, TauaL, TauaR, SaL, SaR, St1aL, St1aR, St2aL, St2aR;
 };
 
-// d(num / den) with den = safe_den(x): adds to a_num and a_x
-__device__ __forceinline__ void div_rev(double g, double q, double sden, double x, double &a_num,
+// d(num / den) with den = safe_den(x), given inv = 1 / den: adds to a_num
+// and a_x
+__device__ __forceinline__ void div_rev(double g, double q, double inv, double x, double &a_num,
                                         double &a_x) {
-    a_num += g / sden;
-    if (live_den(x)) a_x -= g * q / sden;
+    const double gi = g * inv;
+    a_num += gi;
+    if (live_den(x)) a_x -= gi * q;
 }
 
 __device__ __forceinline__ void vars_rev(const double *c, double SL, double SR, double p,
                                          const VarsFwd &v, VarsAdj a, double *ac, double &ap) {
     const double cm = c[R_cm], cx = c[R_cx], ncm = -cm;
     const double BnL = c[R_BnL], BnR = c[R_BnR];
+    // one reciprocal per safe denominator (each is shared by several quotients)
+    const double iXL = 1.0 / v.dXL, iXR = 1.0 / v.dXR, iAL = 1.0 / v.sAL, iAR = 1.0 / v.sAR;
+    const double idL = 1.0 / v.sdL, idR = 1.0 / v.sdR, ill = 1.0 / v.sdll;
     // (FULL part, reversed first)
     const double eL = v.TauaL + v.DaL + p, eR = v.TauaR + v.DaR + p;
     double a_eL = 0, a_eR = 0, a_vBaL = 0, a_vBaR = 0;
@@ -522,14 +526,14 @@ __device__ __forceinline__ void vars_rev(const double *c, double SL, double SR, 
     // Taua = (T + p va - vBa Bn) / sA - Da
     {
         double a_num = 0, a_x = 0;
-        const double q = (c[R_TL] + p * v.vaL - v.vBaL * BnL) / v.sAL;
-        div_rev(a.TauaL, q, v.sAL, v.dAL, a_num, a_x);
+        const double q = (c[R_TL] + p * v.vaL - v.vBaL * BnL) * iAL;
+        div_rev(a.TauaL, q, iAL, v.dAL, a_num, a_x);
         a.DaL -= a.TauaL;
         ac[R_TL] += a_num; ap += a_num * v.vaL; a.vaL += a_num * p; a_vBaL -= a_num * BnL; ac[R_BnL] -= a_num * v.vBaL;
         double a_dAL = a_x;
-        const double qr = (c[R_TR] + p * v.vaR - v.vBaR * BnR) / v.sAR;
+        const double qr = (c[R_TR] + p * v.vaR - v.vBaR * BnR) * iAR;
         double b_num = 0, b_x = 0;
-        div_rev(a.TauaR, qr, v.sAR, v.dAR, b_num, b_x);
+        div_rev(a.TauaR, qr, iAR, v.dAR, b_num, b_x);
         a.DaR -= a.TauaR;
         ac[R_TR] += b_num; ap += b_num * v.vaR; a.vaR += b_num * p; a_vBaR -= b_num * BnR; ac[R_BnR] -= b_num * v.vBaR;
         double a_dAR = b_x;
@@ -540,10 +544,10 @@ __device__ __forceinline__ void vars_rev(const double *c, double SL, double SR, 
         a.vt2aR += a_vBaR * v.Bt2aR; a.Bt2aR += a_vBaR * v.vt2aR;
         // Da = RD / sA
         double c_num = 0;
-        div_rev(a.DaL, v.DaL, v.sAL, v.dAL, c_num, a_dAL);
+        div_rev(a.DaL, v.DaL, iAL, v.dAL, c_num, a_dAL);
         ac[R_DL] += c_num;
         double d_num = 0;
-        div_rev(a.DaR, v.DaR, v.sAR, v.dAR, d_num, a_dAR);
+        div_rev(a.DaR, v.DaR, iAR, v.dAR, d_num, a_dAR);
         ac[R_DR] += d_num;
         // KaLBc / KaRBc / KaL2 / KaR2
         a.KaL += a.KaLBc * BnR; ac[R_BnR] += a.KaLBc * v.KaL; a.Kt1aL += a.KaLBc * v.Bt1c; a.Bt1c += a.KaLBc * v.Kt1aL;
@@ -554,8 +558,8 @@ __device__ __forceinline__ void vars_rev(const double *c, double SL, double SR, 
         a.KaR += 2.0 * a.KaR2 * v.KaR; a.Kt1aR += 2.0 * a.KaR2 * v.Kt1aR; a.Kt2aR += 2.0 * a.KaR2 * v.Kt2aR;
         // Bt{1,2}c = nB / sdll, dll = KaR - KaL
         double a_nB1 = 0, a_nB2 = 0, a_dll = 0;
-        div_rev(a.Bt1c, v.Bt1c, v.sdll, v.dll, a_nB1, a_dll);
-        div_rev(a.Bt2c, v.Bt2c, v.sdll, v.dll, a_nB2, a_dll);
+        div_rev(a.Bt1c, v.Bt1c, ill, v.dll, a_nB1, a_dll);
+        div_rev(a.Bt2c, v.Bt2c, ill, v.dll, a_nB2, a_dll);
         a.KaR += a_dll;
         a.KaL -= a_dll;
         // nB = (Bt_aR (KaR - vaR) + BnR vt_aR) - (Bt_aL (KaL - vaL) + BnL vt_aL)
@@ -569,17 +573,17 @@ __device__ __forceinline__ void vars_rev(const double *c, double SL, double SR, 
         ac[R_BnL] -= a_nB2 * v.vt2aL; a.vt2aL -= a_nB2 * BnL;
         // K vectors: (num) / sd
         double a_dL = 0, a_dR = 0, n;
-        n = 0; div_rev(a.KaL, v.KaL, v.sdL, v.dL, n, a_dL);
+        n = 0; div_rev(a.KaL, v.KaL, idL, v.dL, n, a_dL);
         ac[R_SiL] += n; ap += n; ac[R_BiL] -= n * SL * v.sqL; a.sqL -= n * c[R_BiL] * SL;
-        n = 0; div_rev(a.KaR, v.KaR, v.sdR, v.dR, n, a_dR);
+        n = 0; div_rev(a.KaR, v.KaR, idR, v.dR, n, a_dR);
         ac[R_SiR] += n; ap += n; ac[R_BiR] += n * SR * v.sqR; a.sqR += n * c[R_BiR] * SR;
-        n = 0; div_rev(a.Kt1aL, v.Kt1aL, v.sdL, v.dL, n, a_dL);
+        n = 0; div_rev(a.Kt1aL, v.Kt1aL, idL, v.dL, n, a_dL);
         ac[R_S1L] += n; ac[R_B1L] -= n * SL * v.sqL; a.sqL -= n * c[R_B1L] * SL;
-        n = 0; div_rev(a.Kt1aR, v.Kt1aR, v.sdR, v.dR, n, a_dR);
+        n = 0; div_rev(a.Kt1aR, v.Kt1aR, idR, v.dR, n, a_dR);
         ac[R_S1R] += n; ac[R_B1R] += n * SR * v.sqR; a.sqR += n * c[R_B1R] * SR;
-        n = 0; div_rev(a.Kt2aL, v.Kt2aL, v.sdL, v.dL, n, a_dL);
+        n = 0; div_rev(a.Kt2aL, v.Kt2aL, idL, v.dL, n, a_dL);
         ac[R_S2L] += n; ac[R_B2L] -= n * SL * v.sqL; a.sqL -= n * c[R_B2L] * SL;
-        n = 0; div_rev(a.Kt2aR, v.Kt2aR, v.sdR, v.dR, n, a_dR);
+        n = 0; div_rev(a.Kt2aR, v.Kt2aR, idR, v.dR, n, a_dR);
         ac[R_S2R] += n; ac[R_B2R] += n * SR * v.sqR; a.sqR += n * c[R_B2R] * SR;
         // dL = ncm p + TL - BnL SL sqL; dR = cx p + TR + BnR SR sqR
         ac[R_cm] -= a_dL * p; ap += a_dL * ncm; ac[R_TL] += a_dL; ac[R_BnL] -= a_dL * SL * v.sqL; a.sqL -= a_dL * BnL * SL;
@@ -592,10 +596,10 @@ __device__ __forceinline__ void vars_rev(const double *c, double SL, double SR, 
         double a_vRSL = 0, a_vRSR = 0;
         {
             double nn = 0;
-            div_rev(a_waL, (c[R_TL] - v.vRSL) / v.sAL, v.sAL, v.dAL, nn, a_dAL);
+            div_rev(a_waL, (c[R_TL] - v.vRSL) * iAL, iAL, v.dAL, nn, a_dAL);
             ac[R_TL] += nn; a_vRSL -= nn;
             nn = 0;
-            div_rev(a_waR, (c[R_TR] - v.vRSR) / v.sAR, v.sAR, v.dAR, nn, a_dAR);
+            div_rev(a_waR, (c[R_TR] - v.vRSR) * iAR, iAR, v.dAR, nn, a_dAR);
             ac[R_TR] += nn; a_vRSR -= nn;
         }
         // vRS = va Si + vt1a S1 + vt2a S2
@@ -606,13 +610,13 @@ __device__ __forceinline__ void vars_rev(const double *c, double SL, double SR, 
         // Bt_a = (RB - Bn vt_a) / sA
         {
             double nn = 0;
-            div_rev(a.Bt1aL, v.Bt1aL, v.sAL, v.dAL, nn, a_dAL);
+            div_rev(a.Bt1aL, v.Bt1aL, iAL, v.dAL, nn, a_dAL);
             ac[R_B1L] += nn; ac[R_BnL] -= nn * v.vt1aL; a.vt1aL -= nn * BnL;
-            nn = 0; div_rev(a.Bt2aL, v.Bt2aL, v.sAL, v.dAL, nn, a_dAL);
+            nn = 0; div_rev(a.Bt2aL, v.Bt2aL, iAL, v.dAL, nn, a_dAL);
             ac[R_B2L] += nn; ac[R_BnL] -= nn * v.vt2aL; a.vt2aL -= nn * BnL;
-            nn = 0; div_rev(a.Bt1aR, v.Bt1aR, v.sAR, v.dAR, nn, a_dAR);
+            nn = 0; div_rev(a.Bt1aR, v.Bt1aR, iAR, v.dAR, nn, a_dAR);
             ac[R_B1R] += nn; ac[R_BnR] -= nn * v.vt1aR; a.vt1aR -= nn * BnR;
-            nn = 0; div_rev(a.Bt2aR, v.Bt2aR, v.sAR, v.dAR, nn, a_dAR);
+            nn = 0; div_rev(a.Bt2aR, v.Bt2aR, iAR, v.dAR, nn, a_dAR);
             ac[R_B2R] += nn; ac[R_BnR] -= nn * v.vt2aR; a.vt2aR -= nn * BnR;
         }
         // dA = ncm - va / cx - va
@@ -621,15 +625,15 @@ __device__ __forceinline__ void vars_rev(const double *c, double SL, double SR, 
         // va, vt1a, vt2a = (num) / dX
         double a_XL = 0, a_XR = 0, a_nvaL = 0, a_nvaR = 0, a_QL = 0, a_QR = 0, a_n1L = 0, a_n1R = 0;
         double nn1 = 0;
-        div_rev(a.vaL, v.vaL, v.dXL, v.XL, a_nvaL, a_XL);
-        div_rev(a.vaR, v.vaR, v.dXR, v.XR, a_nvaR, a_XR);
-        nn1 = 0; div_rev(a.vt1aL, v.vt1aL, v.dXL, v.XL, nn1, a_XL);
+        div_rev(a.vaL, v.vaL, iXL, v.XL, a_nvaL, a_XL);
+        div_rev(a.vaR, v.vaR, iXR, v.XR, a_nvaR, a_XR);
+        nn1 = 0; div_rev(a.vt1aL, v.vt1aL, iXL, v.XL, nn1, a_XL);
         a_QL += nn1 * c[R_S1L]; ac[R_S1L] += nn1 * v.QL; ac[R_B1L] += nn1 * v.n1L; a_n1L += nn1 * c[R_B1L];
-        nn1 = 0; div_rev(a.vt2aL, v.vt2aL, v.dXL, v.XL, nn1, a_XL);
+        nn1 = 0; div_rev(a.vt2aL, v.vt2aL, iXL, v.XL, nn1, a_XL);
         a_QL += nn1 * c[R_S2L]; ac[R_S2L] += nn1 * v.QL; ac[R_B2L] += nn1 * v.n1L; a_n1L += nn1 * c[R_B2L];
-        nn1 = 0; div_rev(a.vt1aR, v.vt1aR, v.dXR, v.XR, nn1, a_XR);
+        nn1 = 0; div_rev(a.vt1aR, v.vt1aR, iXR, v.XR, nn1, a_XR);
         a_QR += nn1 * c[R_S1R]; ac[R_S1R] += nn1 * v.QR; ac[R_B1R] += nn1 * v.n1R; a_n1R += nn1 * c[R_B1R];
-        nn1 = 0; div_rev(a.vt2aR, v.vt2aR, v.dXR, v.XR, nn1, a_XR);
+        nn1 = 0; div_rev(a.vt2aR, v.vt2aR, iXR, v.XR, nn1, a_XR);
         a_QR += nn1 * c[R_S2R]; ac[R_S2R] += nn1 * v.QR; ac[R_B2R] += nn1 * v.n1R; a_n1R += nn1 * c[R_B2R];
         // n1 = C + Bn (ncm Si - T) / C + Bn (cx Si - T)
         double a_CL = a_n1L, a_CR = a_n1R;
@@ -873,7 +877,8 @@ __device__ __forceinline__ void hlld_face_vjp(const double *PL, const double *PR
                 }
                 // ucT = nT / sdn, nT = la uaT - faT + p vc - vBc Bc_i
                 double a_nT = 0, a_dn = 0;
-                div_rev(a_ucT, ucT, sdn, dn, a_nT, a_dn);
+                const double isdn = 1.0 / sdn;
+                div_rev(a_ucT, ucT, isdn, dn, a_nT, a_dn);
                 a_la += a_nT * ua[C_TAU];
                 a_ua[C_TAU] += a_nT * la;
                 const double a_faT = -a_nT;
@@ -890,7 +895,7 @@ __device__ __forceinline__ void hlld_face_vjp(const double *PL, const double *PR
                 a_ua[C_D] += a_ucD * rD;
                 const double a_rD = a_ucD * ua[C_D];
                 double a_nrD = 0;
-                div_rev(a_rD, rD, sdn, dn, a_nrD, a_dn);
+                div_rev(a_rD, rD, isdn, dn, a_nrD, a_dn);
                 a_la += a_nrD;
                 if (left) a.vaL -= a_nrD; else a.vaR -= a_nrD;
                 // dn = la - vc
