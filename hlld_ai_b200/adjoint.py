@@ -1,8 +1,9 @@
 """Gradients through many RK+CT steps: the discrete adjoint on the GPU.
 
 ``CheckpointedRun`` runs the FP64 2D step forward for a fixed sequence of
-time steps, keeping the state every ``checkpoint_every`` steps, and runs the
-adjoint backward: each segment is recomputed once from its checkpoint with
+time steps, keeping the state every ``checkpoint_every`` steps (and the
+last segment's step states and tapes), and runs the adjoint backward: each
+earlier segment is recomputed once from its checkpoint with
 ``hlld_adjoint_record_step`` (the step states and each step's tape kept),
 then the steps are reversed one by one with ``hlld_adjoint_reverse_step``,
 the transpose of the step's Jacobian with the
@@ -75,19 +76,30 @@ class CheckpointedRun:
             torch.empty(self._tape_bytes + 256, dtype=torch.uint8, device=self.device)
             for _ in range(self.every)]
         self.checkpoints: list[State2D] = []
+        self._last_states: list[State2D] = []
         self.dts: list[float] = []
 
     # -- forward ----------------------------------------------------------
     def forward(self, state: State2D, dts) -> State2D:
         """Advance a copy of the (synced, FP64) state through dts; returns
-        the final state and keeps the checkpoints."""
+        the final state and keeps the checkpoints.  The last segment -- the
+        one the backward pass starts with -- is recorded as it runs (its
+        states and tapes kept; hlld_adjoint_record_step advances the state
+        exactly as the plain step does), so the backward pass recomputes
+        only the earlier segments: none when checkpoint_every >= len(dts)."""
         self.dts = [float(d) for d in dts]
         s = state.clone()
         self.checkpoints = []
+        self._last_states = []
+        last = ((len(self.dts) - 1) // self.every) * self.every if self.dts else 0
         for i, dt in enumerate(self.dts):
             if i % self.every == 0:
                 self.checkpoints.append(s.clone())
-            self.stepper.step(s, dt, self.scheme)
+            if i >= last:
+                self.record_step(s, dt, i - last)
+                self._last_states.append(s.clone())
+            else:
+                self.stepper.step(s, dt, self.scheme)
         self.final = s
         return s
 
@@ -143,11 +155,16 @@ class CheckpointedRun:
         for seg in range(len(self.checkpoints) - 1, -1, -1):
             i0 = seg * self.every
             i1 = min(i0 + self.every, nsteps)
-            states = [self.checkpoints[seg].clone()]
-            for i in range(i0, i1):
-                s = states[-1].clone()
-                self.record_step(s, self.dts[i], i - i0)
-                states.append(s)
+            if seg == len(self.checkpoints) - 1 and len(self._last_states) == i1 - i0:
+                # recorded by the forward pass
+                states = [self.checkpoints[seg]] + self._last_states
+                self._last_states = []
+            else:
+                states = [self.checkpoints[seg].clone()]
+                for i in range(i0, i1):
+                    s = states[-1].clone()
+                    self.record_step(s, self.dts[i], i - i0)
+                    states.append(s)
             for i in range(i1 - 1, i0 - 1, -1):
                 self.reverse_step(states[i - i0], states[i - i0 + 1], self.dts[i], i - i0, lam)
             del states

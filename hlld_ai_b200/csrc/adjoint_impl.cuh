@@ -15,7 +15,8 @@
 //
 // Reverse of stage s (driver2d.py:382-391 combine + sync):
 //   a. primitive ghost fill (fold the ghost lambdas onto their sources)
-//   b. C2P of the physical cells (Dual<8> Jacobian, IFT on mu)
+//   b. C2P of the physical cells (reverse mode at the recorded root, IFT on
+//      mu: c2p_vjp.cuh)
 //   c. cell-centred B -> faces
 //   d. conserved and face ghost fills
 //   e. RK combine and flux divergence / CT curl -> lambda of the fluxes and
@@ -27,6 +28,7 @@
 //      cells without atomics.
 #pragma once
 
+#include "c2p_vjp.cuh"
 #include "face_vjp.cuh"
 
 namespace hlld {
@@ -354,22 +356,15 @@ __global__ void __launch_bounds__(kThreads) adj_c2p_kernel(const AdjC2PParams p)
     double Bcx = 0.5 * (p.Bxf[c] + p.Bxf[(int64_t)(i + 1) * nyt + j]);
     double Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
     double C[NCONS] = {p.U[0][c], p.U[1][c], p.U[2][c], p.U[3][c], p.U[4][c], Bcx, Bcy, p.U[5][c]};
-    double P[NPRIM], mu = 0.0;
-    if (p.mu_in) mu = p.mu_in[c];
-    else cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P, &mu);
-    using D8 = Dual<NCONS>;
-    D8 Cd[NCONS], Pd[NPRIM];
-#pragma unroll
-    for (int k = 0; k < NCONS; ++k) Cd[k] = D8::var(C[k], k);
-    cons_to_prim_tangent<D8>(Cd, g.gamma, g.atmo_rho, 1e-10, mu, Pd);
-    double lc[NCONS];
-#pragma unroll
-    for (int k = 0; k < NCONS; ++k) {
-        double s = 0.0;
-#pragma unroll
-        for (int m = 0; m < NPRIM; ++m) s += lp[m] * Pd[m].d[k];
-        lc[k] = s;
+    double mu = 0.0;
+    if (p.mu_in) {
+        mu = p.mu_in[c];
+    } else {
+        double P[NPRIM];
+        cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P, &mu);
     }
+    double lc[NCONS];
+    vjp::c2p_vjp(C, g.gamma, g.atmo_rho, mu, lp, lc);
     p.lU[0][c] += lc[C_D];
     p.lU[1][c] += lc[C_SX];
     p.lU[2][c] += lc[C_SY];
