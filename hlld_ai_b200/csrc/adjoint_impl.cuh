@@ -301,28 +301,41 @@ __global__ void __launch_bounds__(kThreads) adj_sweep_gather_kernel(const AdjGat
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t ncell = (int64_t)g.nxt * g.nyt;
     const int64_t nface = AXIS == 0 ? (int64_t)(g.nxt + 1) * g.nyt : (int64_t)g.nxt * (g.nyt + 1);
-    if (e < nface) p.lBn[e] += p.lamBn[e];
-    if (e >= ncell) return;
-    const int i = (int)(e / g.nyt), j = (int)(e - (int64_t)i * g.nyt);
-    const int c = AXIS == 0 ? i : j;
-    const int tr = AXIS == 0 ? j : i;
-    const int n = AXIS == 0 ? g.nxt : g.nyt;
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < NW; ++k) {
-        const int f = c + 1 + S - k;
-        if (f < 0 || f > n) continue;
-        const int64_t fe = AXIS == 0 ? (int64_t)f * g.nyt + tr : (int64_t)tr * (g.nyt + 1) + f;
-#pragma unroll
-        for (int v = 0; v < 7; ++v) acc[v] += p.lamS[k * 7 + v][fe];
+    // Every load is issued before the first store: the arrays may alias for
+    // all the compiler knows, so a load after a store would wait for it, and
+    // a chain of read-modify-writes would cost one memory latency each.
+    double bn_old = 0.0, bn_add = 0.0;
+    if (e < nface) {
+        bn_old = p.lBn[e];
+        bn_add = p.lamBn[e];
     }
-    p.lP[0][e] += acc[0];
-    p.lP[1][e] += acc[1];
-    p.lP[2][e] += acc[2];
-    p.lP[3][e] += acc[3];
-    p.lP[4][e] += acc[4];
-    p.lP[5][e] += acc[6];
-    p.lBc[e] += acc[5];
+    if (e < ncell) {
+        const int i = (int)(e / g.nyt), j = (int)(e - (int64_t)i * g.nyt);
+        const int c = AXIS == 0 ? i : j;
+        const int tr = AXIS == 0 ? j : i;
+        const int n = AXIS == 0 ? g.nxt : g.nyt;
+        double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            const int f = c + 1 + S - k;
+            if (f < 0 || f > n) continue;
+            const int64_t fe = AXIS == 0 ? (int64_t)f * g.nyt + tr : (int64_t)tr * (g.nyt + 1) + f;
+#pragma unroll
+            for (int v = 0; v < 7; ++v) acc[v] += p.lamS[k * 7 + v][fe];
+        }
+        double old[7];
+#pragma unroll
+        for (int v = 0; v < 6; ++v) old[v] = p.lP[v][e];
+        old[6] = p.lBc[e];
+        p.lP[0][e] = old[0] + acc[0];
+        p.lP[1][e] = old[1] + acc[1];
+        p.lP[2][e] = old[2] + acc[2];
+        p.lP[3][e] = old[3] + acc[3];
+        p.lP[4][e] = old[4] + acc[4];
+        p.lP[5][e] = old[5] + acc[6];
+        p.lBc[e] = old[6] + acc[5];
+    }
+    if (e < nface) p.lBn[e] = bn_old + bn_add;
 }
 
 // ── C2P of the physical cells (c2p_cells_kernel) in reverse ──────────────
@@ -344,35 +357,43 @@ __global__ void __launch_bounds__(kThreads) adj_c2p_kernel(const AdjC2PParams p)
     const int i = g.ng + (int)(e / g.ny), j = g.ng + (int)(e % g.ny);
     const int nyt = g.nyt;
     const int64_t c = (int64_t)i * nyt + j;
+    // Loads before stores throughout (the arrays may alias for all the
+    // compiler knows, so a load after a store waits for it): the primitive
+    // lambdas, and -- for a cell with work -- the state, the root and the
+    // accumulators, then the zeroing and the sums.
     double lp[NPRIM];
     bool any = false;
 #pragma unroll
     for (int k = 0; k < NPRIM; ++k) {
         lp[k] = p.lP[k][c];
-        p.lP[k][c] = 0.0;
         any = any || (lp[k] != 0.0);
     }
-    if (!any) return;
+    if (!any) return;  // nothing to pull back, nothing to zero
     double Bcx = 0.5 * (p.Bxf[c] + p.Bxf[(int64_t)(i + 1) * nyt + j]);
     double Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
     double C[NCONS] = {p.U[0][c], p.U[1][c], p.U[2][c], p.U[3][c], p.U[4][c], Bcx, Bcy, p.U[5][c]};
-    double mu = 0.0;
-    if (p.mu_in) {
-        mu = p.mu_in[c];
-    } else {
+    double mu = p.mu_in ? p.mu_in[c] : 0.0;
+    double acc[8];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] = p.lU[k][c];
+    acc[6] = p.lBcx[c];
+    acc[7] = p.lBcy[c];
+#pragma unroll
+    for (int k = 0; k < NPRIM; ++k) p.lP[k][c] = 0.0;
+    if (!p.mu_in) {
         double P[NPRIM];
         cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P, &mu);
     }
     double lc[NCONS];
     vjp::c2p_vjp(C, g.gamma, g.atmo_rho, mu, lp, lc);
-    p.lU[0][c] += lc[C_D];
-    p.lU[1][c] += lc[C_SX];
-    p.lU[2][c] += lc[C_SY];
-    p.lU[3][c] += lc[C_SZ];
-    p.lU[4][c] += lc[C_TAU];
-    p.lU[5][c] += lc[C_BZ];
-    p.lBcx[c] += lc[C_BX];
-    p.lBcy[c] += lc[C_BY];
+    p.lU[0][c] = acc[0] + lc[C_D];
+    p.lU[1][c] = acc[1] + lc[C_SX];
+    p.lU[2][c] = acc[2] + lc[C_SY];
+    p.lU[3][c] = acc[3] + lc[C_SZ];
+    p.lU[4][c] = acc[4] + lc[C_TAU];
+    p.lU[5][c] = acc[5] + lc[C_BZ];
+    p.lBcx[c] = acc[6] + lc[C_BX];
+    p.lBcy[c] = acc[7] + lc[C_BY];
 }
 
 // cell-centred B = face averages (ct.py:44-54) in reverse: faces gather
@@ -388,20 +409,22 @@ __global__ void __launch_bounds__(kThreads) adj_bc_faces_kernel(const AdjBcParam
     const int nxt = g.nxt, nyt = g.nyt;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nfx = (int64_t)(nxt + 1) * nyt, nfy = (int64_t)nxt * (nyt + 1);
+    // (loads before stores, as in the gathers above)
+    double sx = 0.0, sy = 0.0, ox = 0.0, oy = 0.0;
     if (e < nfx) {
         const int i = (int)(e / nyt), j = (int)(e - (int64_t)i * nyt);
-        double s = 0.0;
-        if (i >= 1) s += p.lBcx[(int64_t)(i - 1) * nyt + j];
-        if (i < nxt) s += p.lBcx[(int64_t)i * nyt + j];
-        p.lBxf[e] += 0.5 * s;
+        if (i >= 1) sx += p.lBcx[(int64_t)(i - 1) * nyt + j];
+        if (i < nxt) sx += p.lBcx[(int64_t)i * nyt + j];
+        ox = p.lBxf[e];
     }
     if (e < nfy) {
         const int i = (int)(e / (nyt + 1)), j = (int)(e - (int64_t)i * (nyt + 1));
-        double s = 0.0;
-        if (j >= 1) s += p.lBcy[(int64_t)i * nyt + j - 1];
-        if (j < nyt) s += p.lBcy[(int64_t)i * nyt + j];
-        p.lByf[e] += 0.5 * s;
+        if (j >= 1) sy += p.lBcy[(int64_t)i * nyt + j - 1];
+        if (j < nyt) sy += p.lBcy[(int64_t)i * nyt + j];
+        oy = p.lByf[e];
     }
+    if (e < nfx) p.lBxf[e] = ox + 0.5 * sx;
+    if (e < nfy) p.lByf[e] = oy + 0.5 * sy;
 }
 
 // ── ghost fills in reverse ───────────────────────────────────────────────
@@ -510,15 +533,15 @@ __global__ void __launch_bounds__(kThreads) adj_divergence_kernel(const AdjUpdat
     auto cell_upd = [&](int i, int j) {
         return i >= g.ng && i < g.ng + g.nx && j >= g.ng && j < g.ng + g.ny;
     };
+    // (every load before the first store, as in the gathers above)
+    double sx[6] = {0, 0, 0, 0, 0, 0}, sy[6] = {0, 0, 0, 0, 0, 0}, sz = 0.0;
     if (e < nfx) {
         const int f = (int)(e / nyt), j = (int)(e - (int64_t)f * nyt);
         const bool hi = cell_upd(f, j), lo = cell_upd(f - 1, j);
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            double s = 0.0;
-            if (hi) s += p.lU[k][(int64_t)f * nyt + j];
-            if (lo) s -= p.lU[k][(int64_t)(f - 1) * nyt + j];
-            p.lFx[k][e] = p.w2 * s / g.dx;
+            if (hi) sx[k] += p.lU[k][(int64_t)f * nyt + j];
+            if (lo) sx[k] -= p.lU[k][(int64_t)(f - 1) * nyt + j];
         }
     }
     if (e < nfy) {
@@ -526,10 +549,8 @@ __global__ void __launch_bounds__(kThreads) adj_divergence_kernel(const AdjUpdat
         const bool hi = cell_upd(i, f), lo = cell_upd(i, f - 1);
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            double s = 0.0;
-            if (hi) s += p.lU[k][(int64_t)i * nyt + f];
-            if (lo) s -= p.lU[k][(int64_t)i * nyt + f - 1];
-            p.lFy[k][e] = p.w2 * s / g.dy;
+            if (hi) sy[k] += p.lU[k][(int64_t)i * nyt + f];
+            if (lo) sy[k] -= p.lU[k][(int64_t)i * nyt + f - 1];
         }
     }
     if (e < ncr) {
@@ -542,15 +563,22 @@ __global__ void __launch_bounds__(kThreads) adj_divergence_kernel(const AdjUpdat
         auto by_upd = [&](int fi, int fj) {
             return fi >= g.ng && fi < g.ng + g.nx && fj >= g.ng && fj <= g.ng + g.ny;
         };
-        double s = 0.0;
         // Bxf(i, j) += w2 (Ez(i, j) - Ez(i, j+1)) / dy
-        if (j < nyt && bx_upd(i, j)) s += p.lBxf[(int64_t)i * nyt + j] / g.dy;
-        if (j >= 1 && bx_upd(i, j - 1)) s -= p.lBxf[(int64_t)i * nyt + j - 1] / g.dy;
+        if (j < nyt && bx_upd(i, j)) sz += p.lBxf[(int64_t)i * nyt + j] / g.dy;
+        if (j >= 1 && bx_upd(i, j - 1)) sz -= p.lBxf[(int64_t)i * nyt + j - 1] / g.dy;
         // Byf(i, j) += w2 (Ez(i+1, j) - Ez(i, j)) / dx
-        if (i < nxt && by_upd(i, j)) s -= p.lByf[(int64_t)i * (nyt + 1) + j] / g.dx;
-        if (i >= 1 && by_upd(i - 1, j)) s += p.lByf[(int64_t)(i - 1) * (nyt + 1) + j] / g.dx;
-        p.lEz[e] = p.w2 * s;
+        if (i < nxt && by_upd(i, j)) sz -= p.lByf[(int64_t)i * (nyt + 1) + j] / g.dx;
+        if (i >= 1 && by_upd(i - 1, j)) sz += p.lByf[(int64_t)(i - 1) * (nyt + 1) + j] / g.dx;
     }
+    if (e < nfx) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) p.lFx[k][e] = p.w2 * sx[k] / g.dx;
+    }
+    if (e < nfy) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) p.lFy[k][e] = p.w2 * sy[k] / g.dy;
+    }
+    if (e < ncr) p.lEz[e] = p.w2 * sz;
 }
 
 // lambda(U0) += a lambda, lambda(U_s) = b lambda on the updated entries
@@ -561,26 +589,39 @@ __global__ void __launch_bounds__(kThreads) adj_update_scale_kernel(const AdjUpd
     if (e >= (int64_t)(g.nx + 1) * (g.ny + 1)) return;
     const int ii = (int)(e / (g.ny + 1)), jj = (int)(e - (int64_t)ii * (g.ny + 1));
     const int i = g.ng + ii, j = g.ng + jj;
-    if (ii < g.nx && jj < g.ny) {
-        const int64_t c = (int64_t)i * nyt + j;
+    // (every load before the first store, as in the gathers above)
+    const bool cell = ii < g.nx && jj < g.ny, fxl = jj < g.ny, fyl = ii < g.nx;
+    const int64_t c = (int64_t)i * nyt + j, fx = c, fy = (int64_t)i * (nyt + 1) + j;
+    double l[6], l0[6], bx = 0.0, bx0 = 0.0, by = 0.0, by0 = 0.0;
+    if (cell) {
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            const double l = p.lU[k][c];
-            p.lU0[k][c] += p.a * l;
-            p.lU[k][c] = p.b * l;
+            l[k] = p.lU[k][c];
+            l0[k] = p.lU0[k][c];
         }
     }
-    if (jj < g.ny) {
-        const int64_t fx = (int64_t)i * nyt + j;
-        const double l = p.lBxf[fx];
-        p.lBx0[fx] += p.a * l;
-        p.lBxf[fx] = p.b * l;
+    if (fxl) {
+        bx = p.lBxf[fx];
+        bx0 = p.lBx0[fx];
     }
-    if (ii < g.nx) {
-        const int64_t fy = (int64_t)i * (nyt + 1) + j;
-        const double l = p.lByf[fy];
-        p.lBy0[fy] += p.a * l;
-        p.lByf[fy] = p.b * l;
+    if (fyl) {
+        by = p.lByf[fy];
+        by0 = p.lBy0[fy];
+    }
+    if (cell) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            p.lU0[k][c] = l0[k] + p.a * l[k];
+            p.lU[k][c] = p.b * l[k];
+        }
+    }
+    if (fxl) {
+        p.lBx0[fx] = bx0 + p.a * bx;
+        p.lBxf[fx] = p.b * bx;
+    }
+    if (fyl) {
+        p.lBy0[fy] = by0 + p.a * by;
+        p.lByf[fy] = p.b * by;
     }
 }
 
@@ -638,39 +679,48 @@ __global__ void __launch_bounds__(kThreads) adj_emf_kernel(const AdjEmfParams p)
     const int64_t nfx = (int64_t)(nxt + 1) * nyt, nfy = (int64_t)nxt * (nyt + 1),
                   nc = (int64_t)nxt * nyt;
     auto lez = [&](int i, int j) { return p.lEz[(int64_t)i * (nyt + 1) + j]; };
+    // (every load before the first store, as in the gathers above)
     // x faces: Ezxf = -FxBt(i, j) at corner (i, j), Ezxfm at corner (i, j + 1)
+    double sx = 0.0, sy = 0.0;
     if (e < nfx) {
         const int i = (int)(e / nyt), j = (int)(e - (int64_t)i * nyt);
-        double s = 0.0;
-        if (emf_live(g, i, j)) s += lez(i, j) * emf_coef(p, i, j).xf;
-        if (emf_live(g, i, j + 1)) s += lez(i, j + 1) * emf_coef(p, i, j + 1).xfm;
-        p.lFxBt[e] = -s;
+        if (emf_live(g, i, j)) sx += lez(i, j) * emf_coef(p, i, j).xf;
+        if (emf_live(g, i, j + 1)) sx += lez(i, j + 1) * emf_coef(p, i, j + 1).xfm;
     }
     // y faces: Ezyf = FyBt(i, j) at corner (i, j), Ezyfm at corner (i + 1, j)
     if (e < nfy) {
         const int i = (int)(e / (nyt + 1)), j = (int)(e - (int64_t)i * (nyt + 1));
-        double s = 0.0;
-        if (emf_live(g, i, j)) s += lez(i, j) * emf_coef(p, i, j).yf;
-        if (emf_live(g, i + 1, j)) s += lez(i + 1, j) * emf_coef(p, i + 1, j).yfm;
-        p.lFyBt[e] = s;
+        if (emf_live(g, i, j)) sy += lez(i, j) * emf_coef(p, i, j).yf;
+        if (emf_live(g, i + 1, j)) sy += lez(i + 1, j) * emf_coef(p, i + 1, j).yfm;
     }
     // cells: E(i, j) is NE of corner (i, j), NW of (i+1, j), SE of (i, j+1),
     // SW of (i+1, j+1); E = Bcx vy - Bcy vx (cell_emf)
+    double lE = 0.0, Bcx = 0.0, Bcy = 0.0, vx = 0.0, vy = 0.0;
+    double o_vy = 0.0, o_vx = 0.0, o_bx = 0.0, o_by = 0.0;
     if (e < nc && p.upwind) {
         const int i = (int)(e / nyt), j = (int)(e - (int64_t)i * nyt);
-        double lE = 0.0;
         if (emf_live(g, i, j)) lE += lez(i, j) * emf_coef(p, i, j).NE;
         if (emf_live(g, i + 1, j)) lE += lez(i + 1, j) * emf_coef(p, i + 1, j).NW;
         if (emf_live(g, i, j + 1)) lE += lez(i, j + 1) * emf_coef(p, i, j + 1).SE;
         if (emf_live(g, i + 1, j + 1)) lE += lez(i + 1, j + 1) * emf_coef(p, i + 1, j + 1).SW;
         if (lE != 0.0) {
-            const double Bcx = 0.5 * (p.Bxf[(int64_t)i * nyt + j] + p.Bxf[(int64_t)(i + 1) * nyt + j]);
-            const double Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
-            p.lvy[e] += Bcx * lE;
-            p.lvx[e] -= Bcy * lE;
-            p.lBcx[e] += p.vy[e] * lE;
-            p.lBcy[e] -= p.vx[e] * lE;
+            Bcx = 0.5 * (p.Bxf[(int64_t)i * nyt + j] + p.Bxf[(int64_t)(i + 1) * nyt + j]);
+            Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
+            vx = p.vx[e];
+            vy = p.vy[e];
+            o_vy = p.lvy[e];
+            o_vx = p.lvx[e];
+            o_bx = p.lBcx[e];
+            o_by = p.lBcy[e];
         }
+    }
+    if (e < nfx) p.lFxBt[e] = -sx;
+    if (e < nfy) p.lFyBt[e] = sy;
+    if (lE != 0.0) {
+        p.lvy[e] = o_vy + Bcx * lE;
+        p.lvx[e] = o_vx - Bcy * lE;
+        p.lBcx[e] = o_bx + vy * lE;
+        p.lBcy[e] = o_by - vx * lE;
     }
 }
 
