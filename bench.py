@@ -650,7 +650,15 @@ def run_adjoint(a):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
     case = RotorCase(n=a.adjoint_n, steps=a.adjoint_steps, checkpoint_every=a.adjoint_every)
-    runs = [rotor_gradients(case, device=dev) for _ in range(max(1, a.steps))]
+    runs = []
+    for _ in range(max(1, a.steps)):
+        r = rotor_gradients(case, device=dev)
+        # keep the numbers only: the run's checkpoints and tapes are freed
+        # before the next run allocates its own
+        runs.append({k: r[k] for k in ("forward_ms", "adjoint_ms", "J", "grad_omega")})
+        del r
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
     ratios = [r["adjoint_ms"] / r["forward_ms"] for r in runs]
     if world > 1:
         m = torch.tensor([max(ratios)], dtype=torch.float64, device=dev)

@@ -1024,9 +1024,16 @@ __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
             double dt = isnan(mx) ? mx : (1.0 / clamp_lo(mx, 1e-14)) * (p.cfl * dx);
             if (dt > p.tend - t) dt = p.tend - t;
             if (!(dt > 0.0)) break;
-            for (int c = threadIdx.x; c < nt; c += blockDim.x)
+            // (each thread loads all it needs before its first store: the
+            // arrays may alias for all the compiler knows, so a load after a
+            // store would wait for it, one memory latency per variable)
+            for (int c = threadIdx.x; c < nt; c += blockDim.x) {
+                double u[8];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) p.U0[k][base + c] = p.U[k][base + c];
+                for (int k = 0; k < 8; ++k) u[k] = p.U[k][base + c];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) p.U0[k][base + c] = u[k];
+            }
             for (int st = 0; st < nst; ++st) {
                 const double *w = p.scheme == 3 ? kRK3d[st] : kRK2d[st];
                 const double w2 = w[2] * dt;
@@ -1042,27 +1049,38 @@ __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
                 // Heun (driver.py:223-232): U1 = U + dt L(U); U' = 0.5 (U + U1 + dt L(U1)),
                 // with rhs = (F_c - F_c+1) / dx on the physical cells; Bx held
                 for (int c = ng + threadIdx.x; DRV && c < ng + L; c += blockDim.x) {
+                    const int64_t ci = base + c;
+                    double rhs[8], u0[8], u[8];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
                         if (k == C_BX) continue;
-                        const double rhs = (double)((p.F[k][fbase + c] - p.F[k][fbase + c + 1]) / R(dx));
-                        const int64_t ci = base + c;
-                        p.U[k][ci] = st == 0 ? p.U0[k][ci] + dt * rhs
-                                             : 0.5 * (p.U0[k][ci] + p.U[k][ci] + dt * rhs);
+                        rhs[k] = (double)((p.F[k][fbase + c] - p.F[k][fbase + c + 1]) / R(dx));
+                        u0[k] = p.U0[k][ci];
+                        u[k] = p.U[k][ci];
+                    }
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        if (k == C_BX) continue;
+                        p.U[k][ci] = st == 0 ? u0[k] + dt * rhs[k] : 0.5 * (u0[k] + u[k] + dt * rhs[k]);
                     }
                 }
                 for (int c = threadIdx.x; !DRV && c < nt; c += blockDim.x) {
+                    double rhs[8], u0[8], u[8];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        double rhs;
                         if (k == C_BX) {
-                            rhs = -(0.0 - 0.0) / dx + (-0.0);
+                            rhs[k] = -(0.0 - 0.0) / dx + (-0.0);
                         } else {
                             R d = p.F[k][fbase + c + 1] - p.F[k][fbase + c];
-                            rhs = (double)(-d / R(dx)) + (-0.0);
+                            rhs[k] = (double)(-d / R(dx)) + (-0.0);
                         }
-                        double v = w[0] * p.U0[k][base + c] + w[1] * p.U[k][base + c];
-                        p.U[k][base + c] = v + w2 * rhs;
+                        u0[k] = p.U0[k][base + c];
+                        u[k] = p.U[k][base + c];
+                    }
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        double v = w[0] * u0[k] + w[1] * u[k];
+                        p.U[k][base + c] = v + w2 * rhs[k];
                     }
                 }
                 __syncthreads();
@@ -1070,8 +1088,11 @@ __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
                 for (int c = threadIdx.x; c < 2 * ng; c += blockDim.x) {
                     const int gc = c < ng ? c : L + c;
                     const int sc = c < ng ? ng : ng + L - 1;
+                    double u[8];
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) p.U[k][base + gc] = p.U[k][base + sc];
+                    for (int k = 0; k < 8; ++k) u[k] = p.U[k][base + sc];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) p.U[k][base + gc] = u[k];
                 }
                 __syncthreads();
                 for (int c = ng + threadIdx.x; c < ng + L; c += blockDim.x) {
@@ -1086,8 +1107,11 @@ __global__ void __launch_bounds__(256, 2) tubes_kernel(const TubesParams p) {
                 for (int c = threadIdx.x; c < 2 * ng; c += blockDim.x) {
                     const int gc = c < ng ? c : L + c;
                     const int sc = c < ng ? ng : ng + L - 1;
+                    R q[NPRIM];
 #pragma unroll
-                    for (int k = 0; k < NPRIM; ++k) p.P[k][base + gc] = p.P[k][base + sc];
+                    for (int k = 0; k < NPRIM; ++k) q[k] = p.P[k][base + sc];
+#pragma unroll
+                    for (int k = 0; k < NPRIM; ++k) p.P[k][base + gc] = q[k];
                 }
                 __syncthreads();
             }
