@@ -218,9 +218,8 @@ def _timed_rotor(a, precision, dev, world, record=True):
     U0 = [torch.empty(g.nxt * g.nyt, **f64) for _ in range(6)]
     Bx0, By0 = torch.empty(nfx, **f64), torch.empty(nfy, **f64)
     diag = torch.zeros(ctypes.sizeof(_lib.StepDiag), dtype=torch.uint8, device=dev)
-    # the mixed form's C2P and p* roots of the step's first stage (as hlld_rk_step_ct)
+    # the mixed form's C2P roots of the step's first stage (as hlld_rk_step_ct)
     mu = torch.zeros(g.nxt * g.nyt, dtype=torch.float64, device=dev) if precision == "mixed" else None
-    pstar = ([torch.zeros(nfx, **f64), torch.zeros(nfy, **f64)] if precision == "mixed" else None)
     fd_off = ctypes.sizeof(_lib.FluxDiag)
     pFx, pFy, pU0 = _lib.ptr_array(Fx), _lib.ptr_array(Fy), _lib.ptr_array(U0)
     dt = stepper.dt_buf
@@ -234,18 +233,8 @@ def _timed_rotor(a, precision, dev, world, record=True):
                     e0 = torch.cuda.Event(enable_timing=True)
                     e1 = torch.cuda.Event(enable_timing=True)
                     e0.record(stream)
-                if mu is None:
-                    _lib.check(L.hlld_sweep2d(ctypes.byref(gc), ctypes.byref(s), axis, pF,
-                                              diag.data_ptr() + axis * fd_off, sh), "sweep2d")
-                else:
-                    # mixed form, as hlld_rk_step_ct: stage 0 keeps each face's
-                    # p*, the later stages start from it
-                    ps = pstar[axis].data_ptr()
-                    _lib.check(L.hlld_sweep2d_roots(ctypes.byref(gc), ctypes.byref(s), axis, pF,
-                                                    diag.data_ptr() + axis * fd_off,
-                                                    ps if stage == 0 else None,
-                                                    None if stage == 0 else ps, sh),
-                               "sweep2d_roots")
+                _lib.check(L.hlld_sweep2d(ctypes.byref(gc), ctypes.byref(s), axis, pF,
+                                          diag.data_ptr() + axis * fd_off, sh), "sweep2d")
                 if rec:
                     e1.record(stream)
                     sweep_events.append((e0, e1))

@@ -92,8 +92,6 @@ SIGNATURES = {
                                              _VP, _VP, _VP, _VP, _VP]),
     "hlld_sweep2d": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
                                     ctypes.c_int, _PP, _VP, _VP]),
-    "hlld_sweep2d_roots": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
-                                          ctypes.c_int, _PP, _VP, _VP, _VP, _VP]),
     "hlld_ct_update2d": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC), _PP,
                                         _PP, _VP, _PP, _VP, _VP, _VP, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_double, _VP, _VP]),

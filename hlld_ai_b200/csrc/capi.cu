@@ -94,9 +94,6 @@ size_t layout_scratch(const hlld_grid2d_t *g, char *base, hlld::Scratch2D *sc) {
     off += align_up(sizeof(hlld_step_diag_t));
     // mixed form: the C2P roots of the step's first stage (warm start)
     s.mu_warm = g->precision == HLLD_MIXED ? (double *)take(nc, 8) : nullptr;
-    // and the p* of its faces
-    s.ps_x = g->precision == HLLD_MIXED ? (double *)take(nfx, 8) : nullptr;
-    s.ps_y = g->precision == HLLD_MIXED ? (double *)take(nfy, 8) : nullptr;
     if (sc) *sc = s;
     return off;
 }
@@ -248,12 +245,6 @@ int hlld_sync_state_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8
 
 int hlld_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
                  hlld_flux_diag_t *diag, void *stream) {
-    return hlld_sweep2d_roots(g, s, axis, F, diag, nullptr, nullptr, stream);
-}
-
-int hlld_sweep2d_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
-                       hlld_flux_diag_t *diag, double *pstar_out, const double *pstar_start,
-                       void *stream) {
     int rc = check_grid(g);
     if (rc) return rc;
     if ((rc = check_state(s))) return rc;
@@ -264,14 +255,12 @@ int hlld_sweep2d_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis
     cudaStream_t st = (cudaStream_t)stream;
     if (cudaMemsetAsync(diag, 0, sizeof(hlld_flux_diag_t), st) != cudaSuccess)
         return check_launch("sweep2d diag reset");
-    if (pstar_start && g->precision != HLLD_MIXED)
-        return fail(HLLD_ERR_INVALID, "pstar_start is for the mixed form only");
     if (g->precision == HLLD_FP64_EXACT)
-        hlld::v_exact::launch_sweep2d(g, s, axis, F, diag, st, pstar_out);
+        hlld::v_exact::launch_sweep2d(g, s, axis, F, diag, st);
     else if (g->precision == HLLD_MIXED)
-        hlld::v_mixed::launch_sweep2d(g, s, axis, F, diag, st, pstar_out, nullptr, pstar_start);
+        hlld::v_mixed::launch_sweep2d(g, s, axis, F, diag, st);
     else
-        hlld::v_fp64::launch_sweep2d(g, s, axis, F, diag, st, pstar_out);
+        hlld::v_fp64::launch_sweep2d(g, s, axis, F, diag, st);
     return check_launch("sweep2d");
 }
 

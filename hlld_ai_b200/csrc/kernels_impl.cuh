@@ -337,12 +337,9 @@ struct SweepParams {
     const double *Bxf, *Byf;
     R *F[NFLUX];
     hlld_flux_diag_t *diag;
-    // optional per-face record: p* (the adjoint's tape; the mixed step's
-    // later stages start from it) and the HLLE fallback (adjoint)
+    // optional per-face record for the adjoint: p* and the HLLE fallback
     double *pstar_out;
     uint8_t *fail_out;
-    // optional per-face previous root to start the p* solve from (mixed form)
-    const double *pstar_start;
 };
 
 // One face of a directional sweep.  AXIS 0: faces (nxt+1, nyt), face f is
@@ -463,14 +460,13 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
             P[P_BZ] = q[6];
         }
         FaceOut<T> o;
-        const int64_t fi = e;
         if (SOLVER == HLLD_SOLVER_HLLD)
-            hlld_face<AXIS, T, RB, double>(PL, PR, (T)g.gamma, false, o, nullptr,
-                                           p.pstar_start ? p.pstar_start[fi] : 0.0);
+            hlld_face<AXIS, T, RB, double>(PL, PR, (T)g.gamma, false, o);
         else if (SOLVER == HLLD_SOLVER_HLLC)
             hllc_face<AXIS, T>(PL, PR, (T)g.gamma, false, o);
         else
             hlle_face<AXIS, T>(PL, PR, (T)g.gamma, false, false, o);
+        const int64_t fi = e;
         p.F[F_D][fi] = o.F[C_D];
         p.F[F_SX][fi] = o.F[C_SX];
         p.F[F_SY][fi] = o.F[C_SY];
@@ -478,8 +474,10 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         p.F[F_TAU][fi] = o.F[C_TAU];
         p.F[F_BZ][fi] = o.F[C_BZ];
         p.F[F_BT][fi] = AXIS == 0 ? o.F[C_BY] : o.F[C_BX];
-        if (p.pstar_out) p.pstar_out[fi] = (double)o.pstar;
-        if (p.fail_out) p.fail_out[fi] = (o.flags & RF_FAILED) ? 1 : 0;
+        if (p.pstar_out) {
+            p.pstar_out[fi] = (double)o.pstar;
+            p.fail_out[fi] = (o.flags & RF_FAILED) ? 1 : 0;
+        }
         cnt.v[0] = 1;
         cnt.v[1] = o.err > 0;
         cnt.v[2] = (o.flags & RF_WAVE_ORDER_BAD) != 0;
@@ -1313,12 +1311,10 @@ void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t 
 }
 
 void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
-                    hlld_flux_diag_t *fdiag, cudaStream_t st, double *pstar_out, uint8_t *fail_out,
-                    const double *pstar_start) {
+                    hlld_flux_diag_t *fdiag, cudaStream_t st, double *pstar_out, uint8_t *fail_out) {
     SweepParams sp = {};
     sp.pstar_out = pstar_out;
     sp.fail_out = fail_out;
-    sp.pstar_start = pstar_start;
     sp.g = make_grid(g);
     sp.rho = (const R *)s->prims[P_RHO];
     sp.p = (const R *)s->prims[P_P];
@@ -1388,16 +1384,12 @@ void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Sc
         // sweep counters and max |F_D| restart every stage; the CT scale is
         // the current stage's (ct.py:114)
         cudaMemsetAsync(diag, 0, sizeof(hlld_step_diag_t), st);
-        // mixed form: stage 0 solves every face's p* and every cell's C2P in
-        // full and keeps the roots; the later stages of the step start from
-        // them (within the step only, so a step never depends on earlier
-        // calls)
-        const bool first = stage == 0;
-        launch_sweep2d(g, s, 0, sc.Fx, &diag->sweep[0], st, first ? sc.ps_x : nullptr, nullptr,
-                       first ? nullptr : sc.ps_x);
-        launch_sweep2d(g, s, 1, sc.Fy, &diag->sweep[1], st, first ? sc.ps_y : nullptr, nullptr,
-                       first ? nullptr : sc.ps_y);
+        launch_sweep2d(g, s, 0, sc.Fx, &diag->sweep[0], st);
+        launch_sweep2d(g, s, 1, sc.Fy, &diag->sweep[1], st);
         launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
+        // mixed form: stage 0 solves every cell's C2P in full and keeps the
+        // roots; the later stages of the step start from them (within the
+        // step only, so a step never depends on earlier calls)
         if (stage == 0) launch_sync_state(g, s, nullptr, diag, st, sc.mu_warm, nullptr);
         else launch_sync_state(g, s, nullptr, diag, st, nullptr, sc.mu_warm);
     }

@@ -931,37 +931,6 @@ template <typename T> __device__ __forceinline__ T hlld_residual(const HlldR<T> 
     X(RSiL) X(RSiR) X(RS1L) X(RS1R) X(RS2L) X(RS2R) X(RBiL) X(RBiR) X(RB1L) X(RB1R) X(RB2L)      \
     X(RB2R) X(RTL) X(RTR) X(RDL) X(RDR) X(S_L) X(S_R) X(BnL) X(BnR) X(cm) X(cx)
 
-// Started p* solve (used by the mixed-precision form only): a secant on the
-// HLLD residual from a previous root p0 of the same face, x0 = p0 (1 - 1e-7),
-// x1 = p0.  It returns false -- and the caller runs the reference's
-// bracketed solve -- unless it reaches |r| < tol within eight steps at a
-// positive p*.
-template <typename TP>
-__device__ __forceinline__ bool hlld_pstar_warm(const HlldR<TP> &C, TP p0, TP &p_out,
-                                                int32_t &iters) {
-    const TP tol = K<TP>::pstar_tol;
-    TP x0 = p0 * (TP(1) - TP(1e-7)), x1 = p0;
-    TP f0 = hlld_residual(C, x0), f1 = hlld_residual(C, x1);
-#pragma unroll 1
-    for (int it = 0; it < 8; ++it) {
-        if (fabs(f1) < tol) {
-            if (!(x1 > TP(0))) return false;
-            p_out = x1;
-            iters = it;
-            return true;
-        }
-        const TP df = f1 - f0;
-        if (!(fabs(df) > TP(1e-30) * fabs(f1))) return false;
-        const TP x2 = x1 - f1 * (x1 - x0) / df;
-        if (!(x2 > TP(0))) return false;
-        x0 = x1;
-        f0 = f1;
-        x1 = x2;
-        f1 = hlld_residual(C, x2);
-    }
-    return false;
-}
-
 // p* as a dual number at a solved face: p*'s derivative from the
 // implicit-function theorem on the residual, d p* = -(d_x r) / (d_p r), as
 // one Newton step from the root with the value kept at p*.
@@ -985,8 +954,7 @@ template <typename TP> __device__ __forceinline__ TP hlld_ift_root(const HlldR<T
 // computation; the bracket and the secant are skipped.
 template <int IDIR, typename T, typename TC = T, typename TP = T, bool IFT = false>
 __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, bool want_u,
-                                          FaceOut<T> &o, const double *given = nullptr,
-                                          double p_start = 0.0) {
+                                          FaceOut<T> &o, const double *given = nullptr) {
     constexpr int i = IDIR, t1 = (IDIR + 1) % 3, t2 = (IDIR + 2) % 3;
     Phys<T> ph;
     srmhd_fluxes<IDIR>(PL, PR, gamma, ph);
@@ -998,8 +966,40 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         uH[k] = hu(ph.L.f[k], ph.R.f[k], ph.L.u[k], ph.R.u[k], cm, cx);
     }
 
+    // legacy bracket (hlld.py:1253-1263): total pressure of the HLL state
     TP p_hll = TP(0), p_lo = TP(0), p_hi = TP(0);
-    constexpr int Bn = C_BX + i;
+    constexpr int Sn = C_SX + i, Bn = C_BX + i;
+    if constexpr (!IFT) {
+        TC Ch[NCONS], Ph[NPRIM];
+#pragma unroll
+        for (int k = 0; k < NCONS; ++k) Ch[k] = (TC)uH[k];
+        cons_to_prim<TC>(Ch, (TC)gamma, TC(1e-10), TC(1e-10), Ph);
+        TC pp, cs2;
+        eos_press_cs2(Ph[P_EPS], Ph[P_RHO], (TC)gamma, pp, cs2);
+        TC w = lorentz_W(Ph);
+        TC b2 = comp_b2(Ph, w);
+        p_hll = (TP)(pp + TC(0.5) * b2);
+
+        // p0 from the Bn = 0 limit (hlld.py:1265-1287)
+        TP a = (TP)fH[C_TAU] + (TP)fH[C_D];
+        TP b = -(TP)fH[Sn] - (TP)uH[C_TAU] - (TP)uH[C_D];
+        TP cq = (TP)uH[Sn];
+        TP disc = b * b - TP(4) * a * cq;
+        disc = clamp_lo(disc, TP(0));
+        bool abig = fabs(a) > TP(1e-14);
+        TP safe_a = abig ? a : TP(1);
+        TP safe_b = abig ? b : TP(1);
+        TP v_star = abig ? (-b - sqrt(disc)) / (TP(2) * safe_a) : -cq / safe_b;
+        v_star = clamp_hi(clamp_lo(v_star, -(TP(1) - TP(1e-10))), TP(1) - TP(1e-10));
+        TP p0 = (TP)fH[Sn] - ((TP)fH[C_TAU] + (TP)fH[C_D]) * v_star;
+        p0 = clamp_lo(p0, TP(1e-30));
+
+        const T BnL0 = ph.L.u[Bn], BnR0 = ph.R.u[Bn];
+        TP Bn2 = TP(0.5) * ((TP)BnL0 * (TP)BnL0 + (TP)BnR0 * (TP)BnR0);
+        bool use_p0 = (Bn2 / p_hll) < TP(0.1);
+        p_lo = use_p0 ? p0 * TP(0.99) : p_hll * TP(0.99);
+        p_hi = use_p0 ? p0 * TP(1.01) : p_hll * TP(1.01);
+    }
     const T BnL = ph.L.u[Bn], BnR = ph.R.u[Bn];
     bool bn_zero = (fabs(BnL) < T(1e-14)) && (fabs(BnR) < T(1e-14));
 
@@ -1049,45 +1049,7 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         p_star = hlld_ift_root(C, given[0]);
         err = 0;
         iters_used = 0;
-    } else if (p_start > 0.0 && hlld_pstar_warm(C, (TP)p_start, p_star, iters_used)) {
-        // started from a previous root of this face (mixed form): the same
-        // |r| < tol root, without the HLL-state C2P and the bracket
-        err = 0;
-        p_hll = (TP)p_start;  // (only the magnitude of a failed face's p* record)
     } else {
-        {
-            // legacy bracket (hlld.py:1253-1263): total pressure of the HLL state
-            constexpr int Sn = C_SX + i;
-            TC Ch[NCONS], Ph[NPRIM];
-#pragma unroll
-            for (int k = 0; k < NCONS; ++k) Ch[k] = (TC)uH[k];
-            cons_to_prim<TC>(Ch, (TC)gamma, TC(1e-10), TC(1e-10), Ph);
-            TC pp, cs2;
-            eos_press_cs2(Ph[P_EPS], Ph[P_RHO], (TC)gamma, pp, cs2);
-            TC w = lorentz_W(Ph);
-            TC b2 = comp_b2(Ph, w);
-            p_hll = (TP)(pp + TC(0.5) * b2);
-
-            // p0 from the Bn = 0 limit (hlld.py:1265-1287)
-            TP a = (TP)fH[C_TAU] + (TP)fH[C_D];
-            TP b = -(TP)fH[Sn] - (TP)uH[C_TAU] - (TP)uH[C_D];
-            TP cq = (TP)uH[Sn];
-            TP disc = b * b - TP(4) * a * cq;
-            disc = clamp_lo(disc, TP(0));
-            bool abig = fabs(a) > TP(1e-14);
-            TP safe_a = abig ? a : TP(1);
-            TP safe_b = abig ? b : TP(1);
-            TP v_star = abig ? (-b - sqrt(disc)) / (TP(2) * safe_a) : -cq / safe_b;
-            v_star = clamp_hi(clamp_lo(v_star, -(TP(1) - TP(1e-10))), TP(1) - TP(1e-10));
-            TP p0 = (TP)fH[Sn] - ((TP)fH[C_TAU] + (TP)fH[C_D]) * v_star;
-            p0 = clamp_lo(p0, TP(1e-30));
-
-            const T BnL0 = ph.L.u[Bn], BnR0 = ph.R.u[Bn];
-            TP Bn2 = TP(0.5) * ((TP)BnL0 * (TP)BnL0 + (TP)BnR0 * (TP)BnR0);
-            bool use_p0 = (Bn2 / p_hll) < TP(0.1);
-            p_lo = use_p0 ? p0 * TP(0.99) : p_hll * TP(0.99);
-            p_hi = use_p0 ? p0 * TP(1.01) : p_hll * TP(1.01);
-        }
         TP f_lo = hlld_residual(C, p_lo);
         TP f_hi = hlld_residual(C, p_hi);
         // bracket widening (hlld.py:1314-1321)

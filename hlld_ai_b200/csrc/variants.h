@@ -20,7 +20,6 @@ struct Scratch2D {
     double *Bx0, *By0;
     hlld_step_diag_t *diag;  // used when the caller passes none
     double *mu_warm;         // mixed form: each cell's last C2P root (warm start), or NULL
-    double *ps_x, *ps_y;     // mixed form: each face's last p* (warm start), or NULL
 };
 
 #define HLLD_DECLARE_VARIANT(NS)                                                                  \
@@ -44,8 +43,7 @@ struct Scratch2D {
                               double *dt_dev, unsigned long long *work, cudaStream_t st);         \
     void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis,                \
                         void *const *F, hlld_flux_diag_t *fdiag, cudaStream_t st,                 \
-                        double *pstar_out = nullptr, uint8_t *fail_out = nullptr,                 \
-                        const double *pstar_start = nullptr);                                     \
+                        double *pstar_out = nullptr, uint8_t *fail_out = nullptr);                \
     void launch_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,           \
                           void *const *U0, void *const *F, double *t_out, int32_t *steps_out,     \
                           unsigned int *next, int threads, int blocks, cudaStream_t st);          \

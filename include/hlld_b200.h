@@ -234,19 +234,6 @@ int hlld_sync_state_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8
 int hlld_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
                  hlld_flux_diag_t *diag, void *stream);
 
-/* hlld_sweep2d with the face roots: pstar_out (may be NULL) receives each
- * face's HLLD p* (negative where the face fell back to HLLE); pstar_start
- * (HLLD_MIXED only, may be NULL) holds a previous p* of each face to start
- * the root solve from.  hlld_rk_step_ct does the same internally in the
- * mixed form: its first stage solves every face from the reference's
- * bracket (hlld.py:1253-1321) and keeps the roots, its later stages start
- * from them -- a secant from p0 (1 - 1e-7), p0 to the same |r| < 1e-10
- * tolerance (hlld.py:1080), falling back to the bracketed solve if it does
- * not get there within eight steps. */
-int hlld_sweep2d_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
-                       hlld_flux_diag_t *diag, double *pstar_out, const double *pstar_start,
-                       void *stream);
-
 /* Replaces the rest of ct_stage + combine for RK stage `stage` (0-based) of
  * `scheme` (src/physics/driver2d.py:382-391, :440-445; ct.py:57-185;
  * sweep.py:122-135; state.py:77-103): corner EMF, flux divergence, CT face
