@@ -1,7 +1,7 @@
 // Mixed-precision variant: FP32 primitives, reconstruction, physical
-// fluxes, HLL state, HLL-state C2P (the p* bracket seed), star states, corner
-// EMF and flux divergence; FP64 HLLD p* iteration, cell C2P and RK
-// accumulation of the conserved state and the staggered field.
+// fluxes, HLL state, HLL-state C2P (the p* bracket seed), corner EMF and flux
+// divergence; FP64 HLLD p* bracket and iteration, HLLD star states, cell C2P
+// and RK accumulation of the conserved state and the staggered field.
 #define HLLD_NS v_mixed
 #define HLLD_REAL float
 #ifndef HLLD_BRACKET_REAL
