@@ -151,7 +151,10 @@ class _Grid(ctypes.Structure):
                 ("bc_x", ctypes.c_int), ("bc_y", ctypes.c_int),
                 ("limiter", ctypes.c_int), ("solver", ctypes.c_int),
                 ("gamma", ctypes.c_double), ("atmo_rho", ctypes.c_double),
-                ("upwind", ctypes.c_int)]
+                ("upwind", ctypes.c_int), ("emf_mode", ctypes.c_int)]
+
+
+EMF_MODES = {"solver": 0, "hll": 1}
 
 
 class _Diag(ctypes.Structure):
@@ -175,11 +178,12 @@ class Grid2DSpec:
     gamma: float = 5.0 / 3.0
     atmo_rho: float = 1e-10
     upwind: bool = True
+    emf_mode: str = "solver"  # ct.py:63-88 face EMF: "solver" or "hll"
 
     def c(self) -> _Grid:
         return _Grid(self.nx, self.ny, self.ng, self.dx, self.dy, BCS[self.bc_x],
                      BCS[self.bc_y], LIMITERS[self.limiter], SOLVERS[self.solver],
-                     self.gamma, self.atmo_rho, int(self.upwind))
+                     self.gamma, self.atmo_rho, int(self.upwind), EMF_MODES[self.emf_mode])
 
 
 def _state_ptrs(state: dict):

@@ -1312,8 +1312,11 @@ void orc_sync_state(const orc_grid2d *g, double *const *cons, double *Bxf, doubl
 }
 
 /* one directional sweep (sweep.py:30-119): face fluxes for all faces */
+/* sweep.py:30-119; Fbt_hll (may be NULL): the HLL average of the
+ * transverse-B flux per face for emf_mode "hll" (sweep.py:106-119 with
+ * ct.py:63-96 _hll) */
 static void sweep2d(const orc_grid2d *g, const double *const *prims, const double *Bnf, int axis,
-                    double *const *F, orc_step_diag *diag) {
+                    double *const *F, orc_step_diag *diag, double *Fbt_hll) {
     int nxt = g->nx + 2 * g->ng, nyt = g->ny + 2 * g->ng;
     int64_t nf = axis == 0 ? (int64_t)(nxt + 1) * nyt : (int64_t)nxt * (nyt + 1);
     double *L[ORC_NPRIM], *R[ORC_NPRIM], *U[ORC_NCONS];
@@ -1334,6 +1337,19 @@ static void sweep2d(const orc_grid2d *g, const double *const *prims, const doubl
                 F, U, ps, er, it, fl);
     /* sweep.py:99-100 freeze_normal_B */
     memset(F[ORC_BX + axis], 0, sizeof(double) * (size_t)nf);
+    if (Fbt_hll) {
+        const int kb = axis == 0 ? ORC_BY : ORC_BX;
+        for (int64_t f = 0; f < nf; ++f) {
+            double PL[ORC_NPRIM], PR[ORC_NPRIM];
+            for (int k = 0; k < ORC_NPRIM; ++k) {
+                PL[k] = L[k][f];
+                PR[k] = R[k][f];
+            }
+            phys_t ph;
+            compute_srmhd_fluxes(PL, PR, axis, g->gamma, &ph);
+            Fbt_hll[f] = hf(ph.L.f[kb], ph.R.f[kb], ph.L.u[kb], ph.R.u[kb], ph.cmin, ph.cmax);
+        }
+    }
     if (diag) {
         int64_t nnc = 0, nwb = 0, nbz = 0, nfl = 0, isum = 0, nconv = 0, imax = 0;
         for (int64_t f = 0; f < nf; ++f) {
@@ -1411,10 +1427,13 @@ int orc_rk_step_ct(const orc_grid2d *g, double dt, int scheme, double *const *co
         memcpy(pw[ORC_PBX], Bcx, sizeof(double) * (size_t)nc);
         memcpy(pw[ORC_PBY], Bcy, sizeof(double) * (size_t)nc);
         for (int64_t e = 0; e < nc; ++e) Ec[e] = Bcx[e] * pw[ORC_VY][e] - Bcy[e] * pw[ORC_VX][e];
-        sweep2d(g, (const double *const *)pw, Bxf, 0, Fx, diag);
-        sweep2d(g, (const double *const *)pw, Byf, 1, Fy, diag);
-        for (int64_t e = 0; e < nfx; ++e) Efx[e] = -Fx[ORC_BY][e];
-        for (int64_t e = 0; e < nfy; ++e) Efy[e] = Fy[ORC_BX][e];
+        /* ct.py:63-88 face_emf_x / face_emf_y */
+        const int hll = g->emf_mode == 1;
+        sweep2d(g, (const double *const *)pw, Bxf, 0, Fx, diag, hll ? Efx : NULL);
+        sweep2d(g, (const double *const *)pw, Byf, 1, Fy, diag, hll ? Efy : NULL);
+        for (int64_t e = 0; e < nfx; ++e) Efx[e] = -(hll ? Efx[e] : Fx[ORC_BY][e]);
+        if (!hll)
+            for (int64_t e = 0; e < nfy; ++e) Efy[e] = Fy[ORC_BX][e];
         orc_corner_emf(nxt, nyt, Ec, Efx, Efy, Fx[ORC_D], Fy[ORC_D], g->upwind, Ez);
         /* flux divergence + ct_rhs + combine (sweep.py:122-135, ct.py:180-185,
          * state.py:77-103); L is computed on the fly */

@@ -94,6 +94,10 @@ typedef struct {
     double gamma;
     double atmo_rho;
     int upwind;
+    /* face EMF (ct.py:63-88): 0 "solver", the Riemann solver's transverse-B
+     * flux; 1 "hll", the HLL average of the transverse-B flux from the face
+     * states (sweep.py:106-119) */
+    int emf_mode;
 } orc_grid2d;
 
 typedef struct {

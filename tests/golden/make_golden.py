@@ -21,6 +21,10 @@ inputs, the outputs the oracle is pinned against (tests/test_oracle_golden.py):
   hllc.npz     hllc_flux for idir 0-2 on 512 seeded face pairs, a quarter of
                them with zero normal field (``python make_golden.py REF hllc``
                writes only this file)
+  emf_hll.npz  sync_state + two rk_step_ct steps with emf_mode="hll" (the
+               HLL face EMF, ct.py:63-88) of the rotor and the Orszag-Tang
+               vortex, HLLD and HLLE (``python make_golden.py REF emf_hll``
+               writes only this file)
 
 The reference is not needed to run the tests; only this script reads it.
 """
@@ -346,10 +350,67 @@ def make_hllc(ref_root: str) -> None:
     print("hllc.npz written to", HERE)
 
 
+def make_emf_hll(ref_root: str) -> None:
+    """emf_hll.npz: rk_step_ct with emf_mode="hll" (driver2d.py:162-249,
+    ct.py:63-96, sweep.py:106-119)."""
+    sys.dont_write_bytecode = True
+    os.environ.pop("RMHD_PSTAR_METHOD", None)
+    sys.path.insert(0, ref_root)
+    import torch
+    from src.physics.driver2d import compute_dt_2d, prims_to_cons_2d, rk_step_ct, sync_state
+    from src.physics.eos import hybrid_eos
+    from src.physics.grid import Grid2D
+    from src.physics.hlld import hlle_flux
+    from src.physics.initial_data2d import b_from_potential, magnetic_rotor, orszag_tang
+    from src.physics import reconstruction as rec
+    from src.physics.state import EVOLVED_KEYS, State2D
+
+    torch.set_num_threads(4)
+    PK = ("rho", "vx", "vy", "vz", "p", "eps", "Bx", "By", "Bz")
+    out = {}
+    probs = {
+        "rotor": (magnetic_rotor, (-0.5, 0.5), 5 / 3, ("outflow", "outflow"), "mc", "hlld", 16),
+        "ot": (orszag_tang, (0.0, 1.0), 4 / 3, ("periodic", "periodic"), "mc", "hlld", 16),
+        "ot_hlle": (orszag_tang, (0.0, 1.0), 4 / 3, ("periodic", "periodic"), "mc", "hlle", 16),
+    }
+    for name, (build, box, gam, bc, lim, solver, nn) in probs.items():
+        e = hybrid_eos(K=0.0, gamma=gam, gamma_th=gam)
+        gr = Grid2D(box[0], box[1], nn, box[0], box[1], nn, ng=rec.ghosts_needed(lim))
+        prims, Az = build(gr, e)
+        Bxf, Byf = b_from_potential(Az, gr.dx, gr.dy)
+        for k in PK:
+            out[f"{name}_init_{k}"] = prims[k].numpy().copy()
+        out[f"{name}_init_Bxf"] = Bxf.numpy().copy()
+        out[f"{name}_init_Byf"] = Byf.numpy().copy()
+        c = prims_to_cons_2d(prims, gr)
+        st = State2D(cons={k: c[k] for k in EVOLVED_KEYS}, Bxf=Bxf, Byf=Byf, prims=prims)
+        st = sync_state(st, gr, e, *bc)
+        kw = {"flux_fn": hlle_flux} if solver == "hlle" else {}
+        dts = []
+        for _ in range(2):
+            dt = compute_dt_2d(st.prims, gr, e, 0.4)
+            dts.append(dt)
+            st, _ = rk_step_ct(st, gr, e, dt, scheme="rk3", bc_x=bc[0], bc_y=bc[1], limiter=lim,
+                               emf_mode="hll", **kw)
+        out[f"{name}_dt"] = np.array(dts)
+        for k in EVOLVED_KEYS:
+            out[f"{name}_cons_{k}"] = st.cons[k].numpy()
+        for k in PK:
+            out[f"{name}_prims_{k}"] = st.prims[k].numpy()
+        out[f"{name}_Bxf"] = st.Bxf.numpy()
+        out[f"{name}_Byf"] = st.Byf.numpy()
+        out[f"{name}_meta"] = np.array([nn, rec.ghosts_needed(lim), gam, gr.dx, gr.dy])
+    np.savez_compressed(os.path.join(HERE, "emf_hll.npz"), **out)
+    print("emf_hll.npz written to", HERE)
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if len(sys.argv) > 2 and sys.argv[2] == "hllc":
         make_hllc(root)
+    elif len(sys.argv) > 2 and sys.argv[2] == "emf_hll":
+        make_emf_hll(root)
     else:
         main(root)
         make_hllc(root)
+        make_emf_hll(root)

@@ -250,3 +250,41 @@ def test_hllc_matches_reference(idir):
         assert max_rel(z[f"{idir}_F_{k}"], F[k]) < 1e-12, k
         assert max_rel(z[f"{idir}_U_{k}"], U[k]) < 1e-12, k
     assert max_rel(z[f"{idir}_pstar"], ps) < 1e-14
+
+
+@pytest.mark.parametrize("name,bc,solver", [
+    ("rotor", ("outflow", "outflow"), "hlld"),
+    ("ot", ("periodic", "periodic"), "hlld"),
+    ("ot_hlle", ("periodic", "periodic"), "hlle"),
+])
+def test_rk3_ct_steps_with_hll_face_emf_match_reference(name, bc, solver):
+    """rk_step_ct(emf_mode="hll"): the face EMF is the HLL average of the
+    transverse-B flux (ct.py:63-96, sweep.py:106-119), not the solver's."""
+    z = load("emf_hll.npz")
+    n, ng, gam, dx, dy = z[f"{name}_meta"]
+    n, ng = int(n), int(ng)
+    prims = {k: z[f"{name}_init_{k}"].copy() for k in PK}
+    cons = oracle.prim_to_cons(prims)
+    st = {"cons": {k: cons[k].copy() for k in oracle.EVOLVED_KEYS},
+          "Bxf": z[f"{name}_init_Bxf"].copy(), "Byf": z[f"{name}_init_Byf"].copy(),
+          "prims": prims}
+    g = oracle.Grid2DSpec(n, n, ng, float(dx), float(dy), bc[0], bc[1], "mc", solver, float(gam),
+                          emf_mode="hll")
+    oracle.sync_state(g, st)
+    for dt_ref in z[f"{name}_dt"]:
+        oracle.rk_step_ct(g, st, float(dt_ref), "rk3")
+    for k in oracle.EVOLVED_KEYS:
+        assert max_rel(z[f"{name}_cons_{k}"], st["cons"][k]) < 1e-11, k
+    for k in ("Bxf", "Byf"):
+        assert max_rel(z[f"{name}_{k}"], st[k]) < 1e-11, k
+    if solver == "hlle":
+        return  # the HLLE flux is the HLL average wherever both speeds are positive
+    # with HLLD the mode matters: the solver-EMF step differs
+    st2 = {"cons": {k: cons[k].copy() for k in oracle.EVOLVED_KEYS},
+           "Bxf": z[f"{name}_init_Bxf"].copy(), "Byf": z[f"{name}_init_Byf"].copy(),
+           "prims": {k: z[f"{name}_init_{k}"].copy() for k in PK}}
+    g2 = oracle.Grid2DSpec(n, n, ng, float(dx), float(dy), bc[0], bc[1], "mc", solver, float(gam))
+    oracle.sync_state(g2, st2)
+    for dt_ref in z[f"{name}_dt"]:
+        oracle.rk_step_ct(g2, st2, float(dt_ref), "rk3")
+    assert max_rel(z[f"{name}_Bxf"], st2["Bxf"]) > 1e-9
