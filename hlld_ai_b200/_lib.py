@@ -17,6 +17,7 @@ HLLD_OK = 0
 FP64, FP64_EXACT, MIXED = 0, 1, 2
 PRECISIONS = {"fp64": FP64, "fp64_exact": FP64_EXACT, "mixed": MIXED}
 SOLVERS = {"hlle": 0, "hlld": 1, "hllc": 2}
+EMF_MODES = {"solver": 0, "hll": 1}
 LIMITERS = {"pcm": 0, "mc": 1, "minmod": 2, "weno5z": 3, "mp5": 4, "mp7": 5}
 BCS = {"outflow": 0, "periodic": 1}
 
@@ -43,7 +44,8 @@ class Grid2DC(ctypes.Structure):
                 ("bc_x", ctypes.c_int32), ("bc_y", ctypes.c_int32),
                 ("limiter", ctypes.c_int32), ("solver", ctypes.c_int32),
                 ("gamma", ctypes.c_double), ("atmo_rho", ctypes.c_double),
-                ("upwind", ctypes.c_int32), ("precision", ctypes.c_int32)]
+                ("upwind", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("emf_mode", ctypes.c_int32)]
 
 
 class State2DC(ctypes.Structure):

@@ -55,6 +55,8 @@ int check_grid(const hlld_grid2d_t *g) {
     if (!(g->dx > 0.0) || !(g->dy > 0.0)) return fail(HLLD_ERR_INVALID, "dx, dy must be > 0");
     if (!step_precision(g->precision))
         return fail(HLLD_ERR_UNSUPPORTED, "precision %d not available for the 2D step", g->precision);
+    if (g->emf_mode != HLLD_EMF_SOLVER && g->emf_mode != HLLD_EMF_HLL)
+        return fail(HLLD_ERR_INVALID, "emf_mode must be HLLD_EMF_SOLVER or HLLD_EMF_HLL");
     return HLLD_OK;
 }
 
@@ -387,6 +389,8 @@ static int check_adjoint_grid(const hlld_grid2d_t *g) {
         return fail(HLLD_ERR_UNSUPPORTED, "the adjoint is implemented for HLLD_FP64");
     if (g->solver == HLLD_SOLVER_HLLC)
         return fail(HLLD_ERR_UNSUPPORTED, "the adjoint is implemented for HLLE and HLLD");
+    if (g->emf_mode != HLLD_EMF_SOLVER)
+        return fail(HLLD_ERR_UNSUPPORTED, "the adjoint is implemented for emf_mode HLLD_EMF_SOLVER");
     return HLLD_OK;
 }
 

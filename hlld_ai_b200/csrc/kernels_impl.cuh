@@ -325,6 +325,7 @@ struct Grid {
     int nx, ny, ng, nxt, nyt;
     double dx, dy, gamma, atmo_rho;
     int bc_x, bc_y;
+    int emf_hll;  // face EMF from the HLL average (HLLD_EMF_HLL), else the solver's flux
 };
 
 // face flux slots of a sweep: the six evolved fluxes plus the transverse-B
@@ -344,7 +345,7 @@ struct SweepParams {
 
 // One face of a directional sweep.  AXIS 0: faces (nxt+1, nyt), face f is
 // the lower-x face of cell (f, j).  AXIS 1: faces (nxt, nyt+1).
-template <int AXIS, int LIM, int SOLVER>
+template <int AXIS, int LIM, int SOLVER, bool EMF_HLL>
 __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(const SweepParams p) {
     using T = R;
     constexpr int S = Stencil<LIM>::S;
@@ -466,6 +467,15 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
             hllc_face<AXIS, T>(PL, PR, (T)g.gamma, false, o);
         else
             hlle_face<AXIS, T>(PL, PR, (T)g.gamma, false, false, o);
+        if (EMF_HLL) {
+            // emf_mode "hll" (ct.py:63-96, sweep.py:106-119): the transverse-B
+            // flux, which only feeds the face EMF, is the HLL average of the
+            // face states' fluxes instead of the solver's
+            Phys<T> ph;
+            srmhd_fluxes<AXIS>(PL, PR, (T)g.gamma, ph);
+            constexpr int KB = AXIS == 0 ? C_BY : C_BX;
+            o.F[KB] = hf(ph.L.f[KB], ph.R.f[KB], ph.L.u[KB], ph.R.u[KB], ph.cmin, ph.cmax);
+        }
         const int64_t fi = e;
         p.F[F_D][fi] = o.F[C_D];
         p.F[F_SX][fi] = o.F[C_SX];
@@ -1203,18 +1213,27 @@ static Grid make_grid(const hlld_grid2d_t *g) {
     G.atmo_rho = g->atmo_rho;
     G.bc_x = g->bc_x;
     G.bc_y = g->bc_y;
+    G.emf_hll = g->emf_mode == HLLD_EMF_HLL;
     return G;
 }
 
-template <int AXIS, int LIM>
-static void launch_sweep_lim(int solver, const SweepParams &sp, cudaStream_t st) {
+template <int AXIS, int LIM, bool EMF_HLL>
+static void launch_sweep_emf(int solver, const SweepParams &sp, cudaStream_t st) {
     const int64_t nf = AXIS == 0 ? (int64_t)(sp.g.nxt + 1) * sp.g.nyt : (int64_t)sp.g.nxt * (sp.g.nyt + 1);
     if (solver == HLLD_SOLVER_HLLD)
-        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLD><<<grid1d(nf), kThreads, 0, st>>>(sp);
+        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLD, EMF_HLL><<<grid1d(nf), kThreads, 0, st>>>(sp);
     else if (solver == HLLD_SOLVER_HLLC)
-        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLC><<<grid1d(nf), kThreads, 0, st>>>(sp);
+        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLC, EMF_HLL><<<grid1d(nf), kThreads, 0, st>>>(sp);
     else
-        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLE><<<grid1d(nf), kThreads, 0, st>>>(sp);
+        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLE, EMF_HLL><<<grid1d(nf), kThreads, 0, st>>>(sp);
+}
+
+// the HLL face EMF is a separate instantiation, so that the default sweep
+// carries none of its code
+template <int AXIS, int LIM>
+static void launch_sweep_lim(int solver, const SweepParams &sp, cudaStream_t st) {
+    if (sp.g.emf_hll) launch_sweep_emf<AXIS, LIM, true>(solver, sp, st);
+    else launch_sweep_emf<AXIS, LIM, false>(solver, sp, st);
 }
 
 template <int AXIS>

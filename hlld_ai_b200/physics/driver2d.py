@@ -34,8 +34,8 @@ class Stepper2D:
                  precision="fp64"):
         if vel_var != "Wv":
             raise NotImplementedError("the fused sweep reconstructs W v (vel_var='Wv')")
-        if emf_mode != "solver":
-            raise NotImplementedError("the fused CT update uses emf_mode='solver'")
+        if emf_mode not in _lib.EMF_MODES:
+            raise ValueError(f"unknown emf_mode {emf_mode!r} (ct.py:63-88: 'solver' or 'hll')")
         if bc_x not in _lib.BCS or bc_y not in _lib.BCS:
             raise ValueError(f"unknown boundary condition {(bc_x, bc_y)!r}")
         if limiter not in _lib.LIMITERS:
@@ -55,7 +55,8 @@ class Stepper2D:
         self.gc = _lib.Grid2DC(grid.nx, grid.ny, grid.ng, grid.dx, grid.dy, _lib.BCS[bc_x],
                                _lib.BCS[bc_y], _lib.LIMITERS[limiter],
                                _lib.SOLVERS[solver_name(flux_fn)], eos.kernel_gamma(),
-                               float(atmo_rho), int(bool(upwind)), _lib.PRECISIONS[precision])
+                               float(atmo_rho), int(bool(upwind)), _lib.PRECISIONS[precision],
+                               _lib.EMF_MODES[emf_mode])
         nbytes = ctypes.c_size_t(0)
         _lib.check(_lib.lib().hlld_step2d_scratch_bytes(ctypes.byref(self.gc), ctypes.byref(nbytes)),
                    "hlld_step2d_scratch_bytes")

@@ -81,7 +81,7 @@ def parse(argv=None):
     ap.add_argument("--tend", type=float, default=None)
     ap.add_argument("--cfl", type=float, default=0.25)
     ap.add_argument("--solver", default="hlld", choices=SOLVERS)
-    ap.add_argument("--emf-mode", default="solver", choices=["solver"])
+    ap.add_argument("--emf-mode", default="solver", choices=["solver", "hll"])
     ap.add_argument("--limiter", default="mc", choices=["pcm", "mc", "minmod", "weno5z", "mp5", "mp7"])
     ap.add_argument("--no-upwind-emf", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_exact", "mixed"])
@@ -122,7 +122,7 @@ def main(argv=None):
     g, eos, st, spec = setup_problem(a.problem, a.n, limiter=a.limiter, device=a.device,
                                      precision=a.precision)
     stepper = Stepper2D(g, eos, bc_x=bc_x, bc_y=bc_y, flux_fn=a.solver, limiter=a.limiter,
-                        upwind=not a.no_upwind_emf, precision=a.precision)
+                        emf_mode=a.emf_mode, upwind=not a.no_upwind_emf, precision=a.precision)
     gen = 0
     R = None
     if a.restart:

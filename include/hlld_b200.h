@@ -87,6 +87,16 @@ typedef struct {
     unsigned long long speed_max_bits[2]; /* bits of max(|v_d| + c_f), physical cells */
 } hlld_step_diag_t;
 
+/* Face EMF of the constrained transport (src/physics/ct.py:63-88
+ * face_emf_x / face_emf_y; run_2d.py --emf-mode). */
+enum hlld_emf_mode {
+    /* the Riemann solver's transverse-B flux (the reference's default) */
+    HLLD_EMF_SOLVER = 0,
+    /* the HLL average of the transverse-B flux of the face states
+     * (ct.py:91-96 _hll with sweep.py:106-119), whatever the solver */
+    HLLD_EMF_HLL = 1
+};
+
 typedef struct {
     int32_t nx, ny, ng;
     double dx, dy;
@@ -97,6 +107,7 @@ typedef struct {
     double atmo_rho;
     int32_t upwind;       /* Gardiner-Stone upwinded corner EMF (1) or flux-CT (0) */
     int32_t precision;    /* enum hlld_precision */
+    int32_t emf_mode;     /* enum hlld_emf_mode (0, the default, is the reference's default) */
 } hlld_grid2d_t;
 
 /* State2D (src/physics/state.py:54-74) as device pointers.

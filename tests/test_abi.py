@@ -86,11 +86,16 @@ def test_scratch_size_and_argument_errors_without_gpu():
     nxt = 68
     assert n.value >= 8 * (7 * 2 * (nxt + 1) * nxt + 6 * nxt * nxt)
     for bad in (dict(ng=1, limiter=3), dict(nx=2), dict(bc_x=5), dict(solver=7),
-                dict(gamma=1.0), dict(limiter=9), dict(dx=0.0)):
+                dict(gamma=1.0), dict(limiter=9), dict(dx=0.0), dict(emf_mode=2)):
         gb = grid(**bad)
         rc = L.hlld_step2d_scratch_bytes(ctypes.byref(gb), ctypes.byref(n))
         assert rc == _lib.HLLD_OK - 1, bad  # HLLD_ERR_INVALID
         assert L.hlld_last_error_detail()
+    # the adjoint takes the solver's face EMF only
+    ta, sa = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    gh = grid(emf_mode=1)
+    assert L.hlld_step2d_scratch_bytes(ctypes.byref(gh), ctypes.byref(n)) == 0
+    assert L.hlld_adjoint_tape_bytes(ctypes.byref(gh), ctypes.byref(ta), ctypes.byref(sa)) == -3
     gm = grid(precision=9)
     assert L.hlld_step2d_scratch_bytes(ctypes.byref(gm), ctypes.byref(n)) == -3
     s = _lib.State2DC()

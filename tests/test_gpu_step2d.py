@@ -23,7 +23,7 @@ from hlld_ai_b200.physics.state import EVOLVED_KEYS, PRIM_KEYS, State2D
 pytestmark = pytest.mark.gpu
 
 
-def build(problem, nx, ny, limiter="mc", solver="hlld", precision="fp64_exact"):
+def build(problem, nx, ny, limiter="mc", solver="hlld", precision="fp64_exact", emf_mode="solver"):
     spec = PROBLEMS[problem]
     lo, hi = spec["box"]
     ng = ghosts_needed(limiter)
@@ -38,7 +38,8 @@ def build(problem, nx, ny, limiter="mc", solver="hlld", precision="fp64_exact"):
     cons = oracle.prim_to_cons(prims)
     ostate = {"cons": {k: cons[k].copy() for k in EVOLVED_KEYS}, "Bxf": Bxf.copy(),
               "Byf": Byf.copy(), "prims": {k: prims[k].copy() for k in PRIM_KEYS}}
-    og = oracle.Grid2DSpec(nx, ny, ng, gc.dx, gc.dy, bc[0], bc[1], limiter, solver, spec["gamma"])
+    og = oracle.Grid2DSpec(nx, ny, ng, gc.dx, gc.dy, bc[0], bc[1], limiter, solver, spec["gamma"],
+                           emf_mode=emf_mode)
     oracle.sync_state(og, ostate)
     # device state
     g = Grid2D(lo, hi, nx, lo, hi, ny, ng=ng, device="cuda")
@@ -48,7 +49,7 @@ def build(problem, nx, ny, limiter="mc", solver="hlld", precision="fp64_exact"):
     st = State2D(cons={k: gcons[k].contiguous() for k in EVOLVED_KEYS}, Bxf=dev(Bxf),
                  Byf=dev(Byf), prims=gprims)
     stepper = H.Stepper2D(g, eos, bc_x=bc[0], bc_y=bc[1], flux_fn=solver, limiter=limiter,
-                          precision=precision)
+                          precision=precision, emf_mode=emf_mode)
     stepper.sync(st)
     return g, eos, st, stepper, og, ostate
 
@@ -111,6 +112,49 @@ def test_fma_step_close_to_oracle(problem, nx, ny, limiter, solver):
         oracle.rk_step_ct(og, ostate, dt, "rk3")
         stepper.step(st, dt, "rk3")
     compare(st, ostate, exact=False, tol=1e-9)
+
+
+@pytest.mark.parametrize("problem,limiter,solver", [
+    ("rotor", "mc", "hlld"), ("orszag_tang", "mc", "hlld"), ("orszag_tang", "weno5z", "hlle"),
+    ("rotor_tapered", "mc", "hllc")])
+def test_hll_face_emf_exact_step_bitwise_oracle(problem, limiter, solver):
+    """emf_mode "hll" (ct.py:63-96): the face EMF from the HLL average of the
+    transverse-B flux, whatever the solver; bit for bit with the oracle,
+    which is pinned to the reference's rk_step_ct(emf_mode="hll")."""
+    g, eos, st, stepper, og, ostate = build(problem, 32, 32, limiter, solver, "fp64_exact",
+                                            emf_mode="hll")
+    for _ in range(3):
+        dt = oracle.compute_dt_2d(og, ostate["prims"], 0.4)
+        oracle.rk_step_ct(og, ostate, dt, "rk3")
+        stepper.step(st, dt, "rk3")
+        compare(st, ostate, exact=True)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+def test_hll_face_emf_fast_forms_close_to_oracle(precision, tol):
+    g, eos, st, stepper, og, ostate = build("rotor", 32, 32, "mc", "hlld", precision,
+                                            emf_mode="hll")
+    for _ in range(3):
+        dt = oracle.compute_dt_2d(og, ostate["prims"], 0.4)
+        oracle.rk_step_ct(og, ostate, dt, "rk3")
+        stepper.step(st, dt, "rk3")
+    for name in ("Bxf", "Byf"):
+        a, b = getattr(st, name).cpu().numpy(), ostate[name]
+        assert np.abs(a - b).max() <= tol * np.abs(b).max(), name
+    if precision == "fp64":
+        compare(st, ostate, exact=False, tol=tol)
+
+
+def test_hll_face_emf_keeps_div_b_at_roundoff():
+    """reference tests/test_ct.py:262-289 with emf_mode="hll"."""
+    g, eos, st, stepper, og, ostate = build("orszag_tang", 128, 128, "mc", "hlld", "fp64",
+                                            emf_mode="hll")
+    d0 = g.div_b(st.Bxf, st.Byf)[g.phys]
+    for _ in range(5):
+        stepper.step(st, stepper.compute_dt(st, 0.4), "rk3")
+    d1 = g.div_b(st.Bxf, st.Byf)[g.phys]
+    bmax = float(torch.maximum(st.Bxf.abs().max(), st.Byf.abs().max()))
+    assert float((d1 - d0).abs().max()) < 1e-12 * bmax / g.dx
 
 
 def test_rk2_matches_oracle():
