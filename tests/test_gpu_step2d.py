@@ -45,7 +45,9 @@ def build(problem, nx, ny, limiter="mc", solver="hlld", precision="fp64_exact", 
     g = Grid2D(lo, hi, nx, lo, hi, ny, ng=ng, device="cuda")
     dev = lambda a: torch.from_numpy(a).cuda()
     gprims = {k: dev(prims[k]) for k in PRIM_KEYS}
-    gcons = H.prims_to_cons_2d(gprims, g, precision)
+    gcons = H.prims_to_cons_2d(gprims, g, "fp64" if precision == "mixed" else precision)
+    if precision == "mixed":  # FP32 primitives (recomputed by the sync below)
+        gprims = {k: v.float() for k, v in gprims.items()}
     st = State2D(cons={k: gcons[k].contiguous() for k in EVOLVED_KEYS}, Bxf=dev(Bxf),
                  Byf=dev(Byf), prims=gprims)
     stepper = H.Stepper2D(g, eos, bc_x=bc[0], bc_y=bc[1], flux_fn=solver, limiter=limiter,
@@ -130,19 +132,22 @@ def test_hll_face_emf_exact_step_bitwise_oracle(problem, limiter, solver):
         compare(st, ostate, exact=True)
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
-def test_hll_face_emf_fast_forms_close_to_oracle(precision, tol):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_hll_face_emf_fast_forms_close_to_oracle(precision):
+    """The FMA form within 1e-9 relative; the mixed form within 1e-5 in L1
+    (relative) on the faces and the density."""
     g, eos, st, stepper, og, ostate = build("rotor", 32, 32, "mc", "hlld", precision,
                                             emf_mode="hll")
     for _ in range(3):
         dt = oracle.compute_dt_2d(og, ostate["prims"], 0.4)
         oracle.rk_step_ct(og, ostate, dt, "rk3")
         stepper.step(st, dt, "rk3")
-    for name in ("Bxf", "Byf"):
-        a, b = getattr(st, name).cpu().numpy(), ostate[name]
-        assert np.abs(a - b).max() <= tol * np.abs(b).max(), name
     if precision == "fp64":
-        compare(st, ostate, exact=False, tol=tol)
+        compare(st, ostate, exact=False, tol=1e-9)
+        return
+    for a, b in ((st.Bxf, ostate["Bxf"]), (st.Byf, ostate["Byf"]), (st.cons["D"], ostate["cons"]["D"])):
+        a = a.cpu().numpy()
+        assert np.abs(a - b).mean() <= 1e-5 * np.abs(b).mean()
 
 
 def test_hll_face_emf_keeps_div_b_at_roundoff():
