@@ -27,7 +27,6 @@ from __future__ import annotations
 
 import argparse
 import ctypes
-import datetime
 import json
 import os
 import statistics
@@ -190,15 +189,15 @@ def run_reference(a):
 
 # ── our arm ──────────────────────────────────────────────────────────────────
 
-def _timed_rotor(a, precision, dev, world, record=True):
+def _timed_rotor(a, precision, rp, record=True):
     """Set up the rotor at a.n^2 in `precision`, run a.warmup steps, then time
     a.steps steps between CUDA events; returns a dict of results."""
     import torch
-    import torch.distributed as dist
 
     import hlld_ai_b200 as H
-    from hlld_ai_b200 import _lib
+    from hlld_ai_b200 import _lib, replicas
 
+    dev = rp.device
     g, eos, st, spec = H.setup_problem(PROBLEM, a.n, limiter="mc", device=dev,
                                        precision=precision)
     stepper = H.Stepper2D(g, eos, bc_x=spec["bc"][0], bc_y=spec["bc"][1], flux_fn="hlld",
@@ -254,15 +253,13 @@ def _timed_rotor(a, precision, dev, world, record=True):
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(rp)
     clocks = ClockSampler(dev.index or 0) if record else None
     if clocks:
         clocks.start()
         time.sleep(0.3)
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(rp)
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
@@ -270,18 +267,12 @@ def _timed_rotor(a, precision, dev, world, record=True):
         step(rec=True)
     t1.record(stream)
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(rp)
     clk = clocks.stop() if clocks else None
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        m = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        ms = float(m.item())
+    value, ms = replicas.job_rate(rp, g.nx * g.ny * a.steps, t0.elapsed_time(t1))
     sweep_ms = [e0.elapsed_time(e1) for e0, e1 in sweep_events]
     return dict(g=g, eos=eos, st=st, spec=spec, stepper=stepper, ms=ms, sweep_ms=sweep_ms,
-                clocks=clk, faces=(nfx + nfy) / 2.0,
-                value=world * g.nx * g.ny * a.steps / (ms * 1e-3))
+                clocks=clk, faces=(nfx + nfy) / 2.0, value=value)
 
 
 def _l1_mixed_vs_fp64(a, dev, steps):
@@ -330,21 +321,18 @@ def _sweep_traffic(a):
 
 def run_ours(a):
     import torch
-    import torch.distributed as dist
 
     import hlld_ai_b200 as H
     from hlld_ai_b200.physics.state import EVOLVED_KEYS, PRIM_KEYS
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        dist.init_process_group("nccl", device_id=dev,
-                                timeout=datetime.timedelta(seconds=300))
+    from hlld_ai_b200 import replicas
 
-    main = _timed_rotor(a, a.precision, dev, world, record=True)
+    rp = replicas.from_env("cuda")
+    world, rank, local, dev = rp.world, rp.rank, rp.local, rp.device
+    torch.cuda.set_device(local)
+    replicas.init(rp)
+
+    main = _timed_rotor(a, a.precision, rp, record=True)
     g, st, stepper = main["g"], main["st"], main["stepper"]
     ms, zones = main["ms"], g.nx * g.ny
     value = main["value"]
@@ -366,7 +354,7 @@ def run_ours(a):
     if a.precision == "mixed" and not a.no_fp64_arm:
         del main
         torch.cuda.empty_cache()
-        r64 = _timed_rotor(a, "fp64", dev, world, record=False)
+        r64 = _timed_rotor(a, "fp64", rp, record=False)
         fp64_arm = {"value": r64["value"], "ms_per_step": r64["ms"] / a.steps,
                     "mixed_speedup": value / r64["value"]}
         del r64
@@ -394,8 +382,7 @@ def run_ours(a):
         nbytes = sum(h.numel() * h.element_size() for h in host.values())
         ke = max(2, min(a.steps, 5))
         torch.cuda.synchronize(dev)
-        if world > 1:
-            dist.barrier()
+        replicas.barrier(rp)
         # Every step copies the whole state (cons, faces, prims) from pinned
         # host memory and the whole result back.  The two directions run on
         # their own streams so that they overlap (full duplex): the copy-in
@@ -435,12 +422,8 @@ def run_ours(a):
             stream.wait_event(ev)
         e1.record(stream)
         torch.cuda.synchronize(dev)
-        ems = e0.elapsed_time(e1)
-        if world > 1:
-            m = torch.tensor([ems], dtype=torch.float64, device=dev)
-            dist.all_reduce(m, op=dist.ReduceOp.MAX)
-            ems = float(m.item())
-        e2e = {"value": world * zones * ke / (ems * 1e-3), "unit": "zone-updates/s",
+        e2e_rate, ems = replicas.job_rate(rp, zones * ke, e0.elapsed_time(e1))
+        e2e = {"value": e2e_rate, "unit": "zone-updates/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "steps": ke, "path": "Stepper2D.step + compute_dt with pinned host state; copy-in and "
                        "copy-out on their own streams, overlapped"}
@@ -496,9 +479,7 @@ def run_ours(a):
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(rp)
     return 0
 
 
@@ -532,20 +513,16 @@ def run_tubes(a):
     own CFL steps).  value = physical cell-updates (cells x RK3 steps summed
     over tubes) per second."""
     import torch
-    import torch.distributed as dist
 
+    from hlld_ai_b200 import replicas
     from hlld_ai_b200.tubes import TubeBatch, random_tubes
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rp = replicas.from_env("cuda")
+    world, rank, local, dev = rp.world, rp.rank, rp.local, rp.device
     torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        dist.init_process_group("nccl", device_id=dev,
-                                timeout=datetime.timedelta(seconds=300))
+    replicas.init(rp)
     # tubes are independent units: each rank runs its own seeded batch
-    states = random_tubes(a.tubes, seed=20261203 + rank)
+    states = random_tubes(a.tubes, seed=replicas.replica_seed(20261203, rp))
     precision = "mixed" if a.precision == "mixed" else a.precision
     b = TubeBatch(states, limiter="weno5z", solver="hlld", scheme="rk3", precision=precision,
                   device=dev)
@@ -558,8 +535,7 @@ def run_tubes(a):
     for _ in range(a.warmup):
         g.replay()
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(rp)
     clocks = ClockSampler(dev.index or 0)
     clocks.start()
     time.sleep(0.3)
@@ -578,17 +554,12 @@ def run_tubes(a):
         kernel_ms.append(k0.elapsed_time(k1))
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(rp)
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    updates = int((acc * L).sum().item())
-    if world > 1:
-        m = torch.tensor([ms, float(updates)], dtype=torch.float64, device=dev)
-        mx = m.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(m, op=dist.ReduceOp.SUM)
-        ms, updates = float(mx[0].item()), int(m[1].item())
+    # the batches differ per rank: total work over the slowest rank's time
+    (ms,) = replicas.max_over_ranks(rp, e0.elapsed_time(e1))
+    (updates,) = replicas.sum_over_ranks(rp, float((acc * L).sum().item()))
+    updates = int(updates)
     value = updates / (ms * 1e-3)
     # algorithmic bytes per cell-update: per stage read P (7 words, storage
     # precision) and U (7 FP64), write both; stages 2 and 3 also read U0
@@ -618,8 +589,9 @@ def run_tubes(a):
             host[k].copy_(v, non_blocking=True)
     f1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_updates = int((acc * L).sum().item()) * world
-    e2e = {"value": e2e_updates / (f0.elapsed_time(f1) * 1e-3), "unit": "cell-updates/s",
+    (e2e_updates,) = replicas.sum_over_ranks(rp, float((acc * L).sum().item()))
+    (e2e_ms,) = replicas.max_over_ranks(rp, f0.elapsed_time(f1))
+    e2e = {"value": e2e_updates / (e2e_ms * 1e-3), "unit": "cell-updates/s",
            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ke,
            "path": "TubeBatch.launch with pinned host primitives"}
 
@@ -651,9 +623,7 @@ def run_tubes(a):
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(rp)
     return 0
 
 
@@ -669,15 +639,14 @@ def run_adjoint(a):
     events inside rotor_gradients).
     Replicas under torchrun; rank 0 prints."""
     import torch
-    import torch.distributed as dist
+
+    from hlld_ai_b200 import replicas
     from hlld_ai_b200.adjoint import RotorCase, rotor_gradients
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    if world > 1:
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    rp = replicas.from_env("cuda")
+    world, rank, dev = rp.world, rp.rank, rp.device
     torch.cuda.set_device(dev)
+    replicas.init(rp)
     case = RotorCase(n=a.adjoint_n, steps=a.adjoint_steps, checkpoint_every=a.adjoint_every)
     runs = []
     for _ in range(max(1, a.steps)):
@@ -689,11 +658,7 @@ def run_adjoint(a):
         torch.cuda.synchronize(dev)
         torch.cuda.empty_cache()
     ratios = [r["adjoint_ms"] / r["forward_ms"] for r in runs]
-    if world > 1:
-        m = torch.tensor([max(ratios)], dtype=torch.float64, device=dev)
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(rp)
     if rank == 0:
         line = {"metric": "adjoint time / forward time", "value": statistics.median(ratios),
                 "unit": "x",

@@ -926,16 +926,26 @@ __device__ __forceinline__ void hlld_vars(const HlldR<T> &c, T p, HlldV<T> &o) {
     }
 }
 
-// hlld.py:586-602 residual.  Not inlined: the p* solve evaluates it at five
-// call sites (bracket, widening, secant), and one shared body instead of
-// five inlined copies keeps the persistent tube kernel's hot code within the
-// instruction cache (measured on B200: tubes +15 %, the 2D step unchanged).
-template <typename T> __device__ HLLD_NOINLINE T hlld_residual(const HlldR<T> &c, T p) {
+// hlld.py:586-602 residual
+template <typename T> __device__ __forceinline__ T hlld_residual_body(const HlldR<T> &c, T p) {
     HlldV<T> v;
     hlld_vars<false>(c, p, v);
     T denom_R = c.S_R * v.sqR - v.KaRBc;
     T denom_L = c.S_L * v.sqL + v.KaLBc;
     return (v.laL - v.laR) + c.BnL * (sdiv(T(1) - v.KaR2, denom_R) + sdiv(T(1) - v.KaL2, denom_L));
+}
+// For the real types the residual is kept out of line: the p* solve
+// evaluates it at five call sites (bracket, widening, secant), and one
+// shared body instead of five inlined copies keeps the persistent tube
+// kernel's hot code within the instruction cache (measured on B200: tubes
+// +15 %, the 2D step unchanged).  The dual-number uses (one per face, in the
+// derivative code) stay inlined.
+template <typename T> __device__ HLLD_NOINLINE T hlld_residual_ool(const HlldR<T> &c, T p) {
+    return hlld_residual_body(c, p);
+}
+template <typename T> __device__ __forceinline__ T hlld_residual(const HlldR<T> &c, T p) {
+    if constexpr (sizeof(T) <= sizeof(double)) return hlld_residual_ool(c, p);
+    else return hlld_residual_body(c, p);
 }
 
 #define HLLD_R_FIELDS(X)                                                                        \
