@@ -1,0 +1,132 @@
+"""Reductions and symmetries of the fused 2D step, after the reference's
+tests/test_sweep2d.py:67-172 (which exercise its 2D stepper the same way):
+
+* a shock tube along x stays exactly uniform in y;
+* the same tube run along y, built from cyclically relabelled states, is
+  the relabelled x-run to round-off (the in-plane transverse field is a
+  staggered CT field along x and a cell field along y, so the two runs reach
+  the same numbers by different operation orders);
+* the 2D step on a y-uniform tube equals the batched-tube kernel's 1D step
+  (driver2d.rk_step on a ny = 1 grid) to round-off, with the tube kernel's
+  own CFL dt fed to the 2D step.
+"""
+import numpy as np
+import pytest
+import torch
+
+import hlld_ai_b200 as H
+from hlld_ai_b200.physics.grid import Grid2D
+from hlld_ai_b200.physics.reconstruction import ghosts_needed
+from hlld_ai_b200.physics.state import EVOLVED_KEYS, PRIM_KEYS, State2D
+from hlld_ai_b200.tubes import TubeBatch, TubeStates
+
+pytestmark = pytest.mark.gpu
+
+GAMMA = 2.0
+# co-planar relativistic Brio-Wu (the reference's ST1)
+ST1_L = dict(rho=1.0, p=1.0, vx=0.0, vy=0.0, vz=0.0, Bx=0.5, By=1.0, Bz=0.0)
+ST1_R = dict(rho=0.125, p=0.1, vx=0.0, vy=0.0, vz=0.0, Bx=0.5, By=-1.0, Bz=0.0)
+# a generic state: all components non-zero
+GEN_L = dict(rho=1.0, p=1.0, vx=0.2, vy=-0.1, vz=0.15, Bx=0.7, By=0.6, Bz=-0.4)
+GEN_R = dict(rho=0.3, p=0.2, vx=-0.1, vy=0.25, vz=-0.05, Bx=0.7, By=-0.8, Bz=0.3)
+
+
+def cyc(s: dict, n: int = 1) -> dict:
+    """Cyclic relabelling C^n of vector components: i <- (i - n) mod 3."""
+    out = dict(s)
+    for tri in (("vx", "vy", "vz"), ("Bx", "By", "Bz")):
+        for i, k in enumerate(tri):
+            out[k] = s[tri[(i - n) % 3]]
+    return out
+
+
+def tube_2d(n_along, n_across, L, R, direction, limiter, solver, eos):
+    """A 2D grid with the Riemann problem at the middle of `direction`,
+    uniform across (periodic there, outflow along); staggered field from the
+    cell values (the normal component is constant along the tube)."""
+    nx, ny = (n_along, n_across) if direction == "x" else (n_across, n_along)
+    ng = ghosts_needed(limiter)
+    g = Grid2D(0.0, 1.0, nx, 0.0, 1.0, ny, ng=ng, device="cuda")
+    x = (torch.arange(g.nxt, dtype=torch.float64, device="cuda") - ng + 0.5) / nx
+    y = (torch.arange(g.nyt, dtype=torch.float64, device="cuda") - ng + 0.5) / ny
+    X, Y = torch.meshgrid(x, y, indexing="ij")
+    left = (X < 0.5) if direction == "x" else (Y < 0.5)
+    prims = {k: torch.where(left, torch.tensor(L[k], dtype=torch.float64, device="cuda"),
+                            torch.tensor(R[k], dtype=torch.float64, device="cuda")).contiguous()
+             for k in ("rho", "p", "vx", "vy", "vz", "Bx", "By", "Bz")}
+    prims["eps"] = eos.eps__press_rho(prims["p"], prims["rho"])
+    # faces: the cell value of the cell on the face's high side (the normal
+    # field is uniform; the transverse staggered field is uniform across)
+    Bxf = torch.cat([prims["Bx"], prims["Bx"][-1:]], 0).contiguous()
+    Byf = torch.cat([prims["By"], prims["By"][:, -1:]], 1).contiguous()
+    c = H.prims_to_cons_2d(prims, g)
+    st = State2D(cons={k: c[k].contiguous() for k in EVOLVED_KEYS}, Bxf=Bxf, Byf=Byf,
+                 prims={k: prims[k] for k in PRIM_KEYS})
+    bc = ("outflow", "periodic") if direction == "x" else ("periodic", "outflow")
+    stepper = H.Stepper2D(g, eos, bc_x=bc[0], bc_y=bc[1], flux_fn=solver, limiter=limiter,
+                          precision="fp64")
+    stepper.sync(st)
+    return g, st, stepper
+
+
+@pytest.mark.parametrize("limiter", ["pcm", "mc"])
+def test_tube_along_x_stays_uniform_in_y(limiter):
+    eos = H.hybrid_eos(K=0.0, gamma=GAMMA, gamma_th=GAMMA)
+    g, st, stepper = tube_2d(40, 8, ST1_L, ST1_R, "x", limiter, "hlld", eos)
+    for _ in range(15):
+        stepper.step(st, stepper.compute_dt(st, 0.4), "rk3")
+    ph = g.phys
+    for k in ("rho", "p", "vx", "vy", "By", "Bz"):
+        col = st.prims[k][ph]
+        assert float((col - col[:, :1]).abs().max()) == 0.0, k
+
+
+@pytest.mark.parametrize("limiter", ["pcm", "mc", "weno5z"])
+@pytest.mark.parametrize("solver", ["hlle", "hlld"])
+@pytest.mark.parametrize("states", ["st1", "generic"])
+def test_rotated_tube_equals_relabelled_x_tube(limiter, solver, states):
+    eos = H.hybrid_eos(K=0.0, gamma=GAMMA, gamma_th=GAMMA)
+    L, R = (ST1_L, ST1_R) if states == "st1" else (GEN_L, GEN_R)
+    n, dt = 48, 3.0e-3
+    gx, sx, stx = tube_2d(n, 4, L, R, "x", limiter, solver, eos)
+    gy, sy, sty = tube_2d(n, 4, cyc(L), cyc(R), "y", limiter, solver, eos)
+    for _ in range(25):
+        stx.step(sx, dt, "rk3")
+        sty.step(sy, dt, "rk3")
+    back = cyc({k: sy.prims[k] for k in ("rho", "p", "vx", "vy", "vz", "Bx", "By", "Bz")}, 2)
+    worst = 0.0
+    for k in ("rho", "p", "vx", "vy", "vz", "Bx", "By", "Bz"):
+        a = sx.prims[k][gx.phys]
+        b = back[k][gy.phys].T
+        scale = max(float(a.abs().max()), 1e-30)
+        worst = max(worst, float((a - b).abs().max()) / scale)
+    assert worst < 1e-12, worst
+
+
+@pytest.mark.parametrize("limiter,solver", [("weno5z", "hlld"), ("mc", "hlle")])
+def test_2d_step_on_a_uniform_tube_equals_the_tube_kernel(limiter, solver):
+    eos = H.hybrid_eos(K=0.0, gamma=GAMMA, gamma_th=GAMMA)
+    n = 64
+    left = {k: np.array([v]) for k, v in GEN_L.items() if k != "Bx"}
+    right = {k: np.array([v]) for k, v in GEN_R.items() if k != "Bx"}
+    for s in (left, right):
+        s["eps"] = s["p"] / (s["rho"] * (GAMMA - 1.0))
+    tb = TubeBatch(TubeStates(np.array([n]), left, right, np.array([GEN_L["Bx"]])),
+                   limiter=limiter, solver=solver, scheme="rk3", precision="fp64", gamma=GAMMA)
+    g, st, stepper = tube_2d(n, 4, GEN_L, GEN_R, "x", limiter, solver, eos)
+    t = 0.0
+    for k in range(6):
+        # one tube step with its own CFL dt, then the 2D step with that dt
+        tb.launch(tend=10.0, max_steps=1, resume=k > 0)
+        torch.cuda.synchronize()
+        dt = float(tb.t_out[0].item())
+        assert 0.0 < dt < 1.0
+        stepper.step(st, dt, "rk3")
+        t += dt
+    ng = g.ng
+    one = tb.tube(0)
+    for key in ("rho", "p", "vx", "vy", "vz", "By", "Bz"):
+        a = one[key][ng:ng + n]
+        b = st.prims[key][ng:ng + n, ng].cpu().numpy()
+        scale = max(np.abs(a).max(), 1e-30)
+        assert np.abs(a - b).max() <= 1e-12 * scale, (key, np.abs(a - b).max() / scale)
