@@ -9,6 +9,12 @@ tests/test_sweep2d.py:67-172 (which exercise its 2D stepper the same way):
 * the 2D step on a y-uniform tube equals the batched-tube kernel's 1D step
   (driver2d.rk_step on a ny = 1 grid) to round-off, with the tube kernel's
   own CFL dt fed to the 2D step.
+
+"To round-off" is 1e-12 relative with HLLE.  With HLLD the bound is 1e-9:
+its p* secant stops at |r| < 1e-10 (hlld.py:1080), so two runs whose
+inputs differ by round-off take different iteration paths and agree to the
+solver's tolerance, not to round-off.  (The reference's own checks hold at
+1e-12 because its two runs feed the solver identical inputs.)
 """
 import numpy as np
 import pytest
@@ -100,7 +106,7 @@ def test_rotated_tube_equals_relabelled_x_tube(limiter, solver, states):
         b = back[k][gy.phys].T
         scale = max(float(a.abs().max()), 1e-30)
         worst = max(worst, float((a - b).abs().max()) / scale)
-    assert worst < 1e-12, worst
+    assert worst < (1e-9 if solver == "hlld" else 1e-12), worst
 
 
 @pytest.mark.parametrize("limiter,solver", [("weno5z", "hlld"), ("mc", "hlle")])
@@ -129,4 +135,5 @@ def test_2d_step_on_a_uniform_tube_equals_the_tube_kernel(limiter, solver):
         a = one[key][ng:ng + n]
         b = st.prims[key][ng:ng + n, ng].cpu().numpy()
         scale = max(np.abs(a).max(), 1e-30)
-        assert np.abs(a - b).max() <= 1e-12 * scale, (key, np.abs(a - b).max() / scale)
+        tol = 1e-9 if solver == "hlld" else 1e-12
+        assert np.abs(a - b).max() <= tol * scale, (key, np.abs(a - b).max() / scale)
