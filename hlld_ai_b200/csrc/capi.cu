@@ -324,14 +324,15 @@ int hlld_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
             return fail(HLLD_ERR_INVALID, "NULL work array %d", k);
     for (int k = 0; k < 9; ++k)
         if (!prims[k]) return fail(HLLD_ERR_INVALID, "prims[%d] is NULL", k);
-    if (threads <= 0) threads = 256;
-    if (threads % 32 || threads > 256)
-        return fail(HLLD_ERR_INVALID, "threads must be a multiple of 32, at most 256");
+    if (threads <= 0) threads = 512;
+    if (threads % 32 || threads > 512)
+        return fail(HLLD_ERR_INVALID, "threads must be a multiple of 32, at most 512");
     if (blocks <= 0) {
+        // as many CTAs as fit at 128 registers per thread: 512 threads per SM
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        blocks = sms * (256 / threads) * 2;
+        blocks = sms * (512 / threads > 0 ? 512 / threads : 1);
     }
     if (blocks > b->ntubes) blocks = b->ntubes;
     cudaStream_t st = (cudaStream_t)stream;

@@ -197,7 +197,7 @@ class TubeBatch:
         return {k: self.prims[k][a:b].double().cpu().numpy() for k in PRIM_KEYS}
 
     def autotune(self, tend: float, cfl: float = 0.4, sample: int = 256,
-                 shapes=((64, 2), (128, 2), (128, 4), (256, 1), (256, 2))) -> tuple:
+                 shapes=((128, 4), (256, 1), (256, 2), (384, 1), (512, 1))) -> tuple:
         """Pick (threads, CTAs per SM) by timing each candidate on a sample of
         the batch (every n/sample-th tube) to `tend`; stores and returns the
         winner as (threads, blocks)."""

@@ -264,7 +264,8 @@ int hlld_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *cons
  * compute_dt each step, until tend or max_steps (flavor HLLD_TUBE_RK_STEP),
  * or the 1D driver's loop (src/physics/driver.py:388-412 around rk2_step,
  * the other flavors), in ONE persistent launch of
- * `blocks` CTAs of `threads` threads (0 = library defaults).  prims (9
+ * `blocks` CTAs of `threads` threads (a multiple of 32, at most 512; 0 =
+ * library defaults: 512 threads, one CTA per SM).  prims (9
  * arrays, ghosts filled) are read and updated in place; cons (8), U0 (8
  * cell arrays) and F (8 face arrays, slot Bx unused) are work arrays;
  * t_out / steps_out get each tube's final time and step count; next is one
