@@ -244,7 +244,7 @@ template <typename T> struct Kastaun {
     // exactly 2^-k after k halvings, so the batch early stop never fires
     // early).  f_a(mu_lo) is a deterministic function of mu_lo, so the value
     // from the previous iteration is reused instead of re-evaluated.
-    __device__ __forceinline__ T mu_plus_bisect() const {
+    __device__ HLLD_NOINLINE T mu_plus_bisect() const {  // (a rare fallback: kept out of the hot code)
         T lo = T(0), hi = T(1) / (T(1) + K<T>::tiny);
         T f_lo = fa(lo);
 #pragma unroll 1
@@ -280,6 +280,38 @@ template <typename T> struct Kastaun {
     // in the reference.  Anything outside these conditions runs the plain
     // loop.  The result is the plain loop's bit for bit.
     __device__ __forceinline__ T mu_plus() const {
+        if constexpr (sizeof(T) == 4) {
+            // FP32 (the mixed form's HLL-state C2P, which only seeds the p*
+            // bracket): the root by the same safeguarded Newton, stopped at a
+            // relative step of 2e-7 (the 24 FP32 halvings resolve 6e-8),
+            // moved just above the root and checked to bound it from above,
+            // f_a(mu+) >= 0; the bisection's answer where the check fails.
+            if (!(rNorm2 < T(1e12)) || !(BtNorm2 < T(1e30)) || !(fa(T(0)) < T(0)))
+                return mu_plus_bisect();
+            const T b = BtNorm2, c = B_dot_r * B_dot_r, rN = rNorm2;
+            T m0 = T(0), m1 = T(1);
+            T mu = T(1) / sqrt(T(1) + rN);
+#pragma unroll 1
+            for (int it = 0; it < 30; ++it) {
+                T ch = T(1) / (T(1) + mu * b);
+                T dch = -b * ch * ch;
+                T rb = rN * ch * ch + mu * ch * (T(1) + ch) * c;
+                T drb = rN * T(2) * ch * dch + c * ((ch + mu * dch) * (T(1) + ch) + mu * ch * dch);
+                T g = mu * mu * (T(1) + rb) - T(1);
+                T dg = T(2) * mu * (T(1) + rb) + mu * mu * drb;
+                if (g < T(0)) m0 = mu;
+                else m1 = mu;
+                if (g == T(0)) break;
+                T nm = mu - g / dg;
+                if (!(nm > m0 && nm < m1)) nm = T(0.5) * (m0 + m1);
+                T stp = fabs(nm - mu);
+                mu = nm;
+                if (stp <= T(2e-7) * mu) break;
+            }
+            const T hi = mu * (T(1) + T(1e-6));
+            if (!(hi > T(0)) || !(fa(hi) >= T(0))) return mu_plus_bisect();
+            return hi;
+        }
         if constexpr (sizeof(T) == 8) {
             if (!(rNorm2 < T(1e12)) || !(BtNorm2 < (T(1) / K<T>::tiny)) || !(fa(T(0)) < T(0)))
                 return mu_plus_bisect();
