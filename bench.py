@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--no-fp64-arm", action="store_true",
                     help="skip timing the FP64 step and the mixed-vs-FP64 L1 check")
     ap.add_argument("--cfl", type=float, default=0.4)
-    ap.add_argument("--cpu-n", type=int, default=512, help="grid of the CPU baseline sample")
+    ap.add_argument("--cpu-n", type=int, default=1024, help="grid of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--tubes", type=int, default=4096)
     ap.add_argument("--chunk", type=float, default=0.01,
                     help="tubes: simulated time every tube advances per step")
-    ap.add_argument("--cpu-tubes", type=int, default=12, help="tubes of the CPU baseline sample")
+    ap.add_argument("--cpu-tubes", type=int, default=30, help="tubes of the CPU baseline sample")
     return ap.parse_args()
 
 
@@ -312,6 +312,12 @@ def _l1_mixed_vs_fp64(a, dev, steps):
 _SWEEP_DRAM_BYTES_PER_FACE_MIXED = (136.3e6 + 133.7e6) / 2 / 2373140
 
 
+# DRAM bytes (read + write) of one mixed-precision tubes_kernel launch
+# measured by ncu (2048 seeded tubes, chunk 0.0005: 5.88 + 9.84 GB over
+# 2.129e7 cell-updates), per cell-update; a launch is scaled by its updates
+_TUBES_DRAM_BYTES_PER_UPDATE_MIXED = (5.876e9 + 9.840e9) / 2.129e7
+
+
 def _sweep_traffic(a):
     if a.precision != "mixed":
         return None
@@ -445,10 +451,11 @@ def run_ours(a):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cpu_sample(a.cpu_n, 1, threads)
-        times = cpu_sample(a.cpu_n, 3, threads)
+        times = cpu_sample(a.cpu_n, 6, threads)  # ~10 s of CPU work at 1024^2
         cpu = {"value": a.cpu_n ** 2 * len(times) / sum(times), "unit": "zone-updates/s",
                "cores": threads, "kind": "port",
-               "sample": f"3 RK3 steps of the same rotor at {a.cpu_n}^2 (C oracle, FP64, {threads} threads)"}
+               "sample": f"{len(times)} RK3 steps of the same rotor at {a.cpu_n}^2, after one "
+                         f"untimed step (C oracle, FP64, {threads} threads)"}
 
     if rank == 0:
         line = {
@@ -613,7 +620,13 @@ def run_tubes(a):
             "gpu_launches": a.steps,
             "roofline": {"bound": "hbm", "kernel": "tubes_kernel", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "traffic": (_TUBES_DRAM_BYTES_PER_UPDATE_MIXED * updates / world / a.steps
+                                     if precision == "mixed" else None),
+                         "traffic_unit": "bytes per launch",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                           "the mixed launch on 2048 tubes, scaled by "
+                                           "cell-updates",
                          "bytes_per_cell_update": bytes_per_update,
                          "avg_launch_ms": kernel_s * 1e3},
             "cpu_baseline": cpu,
