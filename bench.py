@@ -217,7 +217,8 @@ def _timed_rotor(a, precision, rp, record=True):
     U0 = [torch.empty(g.nxt * g.nyt, **f64) for _ in range(6)]
     Bx0, By0 = torch.empty(nfx, **f64), torch.empty(nfy, **f64)
     diag = torch.zeros(ctypes.sizeof(_lib.StepDiag), dtype=torch.uint8, device=dev)
-    # the mixed form's C2P roots of the step's first stage (as hlld_rk_step_ct)
+    # the mixed form's C2P roots of the step's first stage (as hlld_rk_step_ct:
+    # stage 1 starts from the input primitives, stages 2 and 3 from its roots)
     mu = torch.zeros(g.nxt * g.nyt, dtype=torch.float64, device=dev) if precision == "mixed" else None
     fd_off = ctypes.sizeof(_lib.FluxDiag)
     pFx, pFy, pU0 = _lib.ptr_array(Fx), _lib.ptr_array(Fy), _lib.ptr_array(U0)
@@ -244,10 +245,13 @@ def _timed_rotor(a, precision, rp, record=True):
             if mu is None:
                 _lib.check(L.hlld_sync_state(ctypes.byref(gc), ctypes.byref(s), None, None, sh),
                            "sync_state")
-            else:
+            elif stage == 0:  # C2P started from the step's input primitives
+                _lib.check(L.hlld_sync_state_from_prims(ctypes.byref(gc), ctypes.byref(s), None,
+                                                        None, mu.data_ptr(), sh),
+                           "sync_state_from_prims")
+            else:  # started from the roots of stage 1
                 _lib.check(L.hlld_sync_state_roots(ctypes.byref(gc), ctypes.byref(s), None, None,
-                                                   mu.data_ptr() if stage == 0 else None,
-                                                   None if stage == 0 else mu.data_ptr(), sh),
+                                                   None, mu.data_ptr(), sh),
                            "sync_state_roots")
 
     for _ in range(a.warmup):

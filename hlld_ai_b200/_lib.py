@@ -92,6 +92,8 @@ SIGNATURES = {
                                        _VP, _VP]),
     "hlld_sync_state_roots": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
                                              _VP, _VP, _VP, _VP, _VP]),
+    "hlld_sync_state_from_prims": (ctypes.c_int, [ctypes.POINTER(Grid2DC),
+                                                  ctypes.POINTER(State2DC), _VP, _VP, _VP, _VP]),
     "hlld_sweep2d": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
                                     ctypes.c_int, _PP, _VP, _VP]),
     "hlld_ct_update2d": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC), _PP,

@@ -245,6 +245,20 @@ int hlld_sync_state_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8
     return check_launch("sync_state_roots");
 }
 
+int hlld_sync_state_from_prims(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
+                               hlld_step_diag_t *diag, double *mu_out, void *stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_state(s))) return rc;
+    if (g->precision != HLLD_MIXED)
+        return fail(HLLD_ERR_UNSUPPORTED, "the C2P warm start belongs to the mixed form");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (diag && cudaMemsetAsync(diag, 0, sizeof(hlld_step_diag_t), st) != cudaSuccess)
+        return check_launch("sync_state diag reset");
+    hlld::v_mixed::launch_sync_state(g, s, status, diag, st, mu_out, nullptr, true);
+    return check_launch("sync_state_from_prims");
+}
+
 int hlld_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void *const *F,
                  hlld_flux_diag_t *diag, void *stream) {
     int rc = check_grid(g);

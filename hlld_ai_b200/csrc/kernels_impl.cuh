@@ -717,8 +717,22 @@ struct C2PCellsParams {
     double *mu_warm; // optional per-cell previous root, read as the start and updated
 };
 
+// Kastaun's root mu = 1 / (h W) of a cell's primitives (h = 1 + eps + p / rho),
+// or 0 -- no start, the bracketed solve -- where they are not physical
+__device__ __forceinline__ double kastaun_mu_of_prims(const R *const *P, int64_t c) {
+    const double rho = P[P_RHO][c], press = P[P_P][c], eps = P[P_EPS][c];
+    const double vx = P[P_VX][c], vy = P[P_VY][c], vz = P[P_VZ][c];
+    const double v2 = vx * vx + vy * vy + vz * vz;
+    const double h = 1.0 + eps + press / rho;
+    return (v2 < 1.0 && rho > 0.0 && h > 0.0) ? sqrt(1.0 - v2) / h : 0.0;
+}
+
 // cell-centred B (ct.py:44-54) + C2P (c2p.py:313-363) of the physical cells,
-// in double; primitives stored as R
+// in double; primitives stored as R.  FROM_PRIMS: each root search starts
+// from the root of the cell's current primitives, which the kernel then
+// overwrites (a template flag: a runtime one made the other launches 5 %
+// slower)
+template <bool FROM_PRIMS>
 __global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParams p) {
     const Grid &g = p.g;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -732,7 +746,9 @@ __global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParam
         double C[NCONS] = {p.U[0][c], p.U[1][c], p.U[2][c], p.U[3][c], p.U[4][c], Bcx, Bcy, p.U[5][c]};
         double P[NPRIM];
         double mu = 0.0;
-        const double mu0 = p.mu_warm ? p.mu_warm[c] : 0.0;
+        double mu0 = 0.0;
+        if constexpr (FROM_PRIMS) mu0 = kastaun_mu_of_prims(p.P, c);
+        else if (p.mu_warm) mu0 = p.mu_warm[c];
         uint8_t st = cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P,
                                           (p.mu_out || p.mu_warm) ? &mu : nullptr, mu0);
         if (p.mu_out) p.mu_out[c] = mu;
@@ -1311,7 +1327,8 @@ static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStre
 }
 
 void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
-                       hlld_step_diag_t *diag, cudaStream_t st, double *mu_out, double *mu_warm) {
+                       hlld_step_diag_t *diag, cudaStream_t st, double *mu_out, double *mu_warm,
+                       bool start_from_prims) {
     Grid G = make_grid(g);
     double *cons[6];
     for (int k = 0; k < 6; ++k) cons[k] = (double *)s->cons[k];
@@ -1329,7 +1346,10 @@ void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t 
     cp.diag = diag;
     cp.mu_out = mu_out;
     cp.mu_warm = mu_warm;
-    c2p_cells_kernel<<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(cp);
+    if (start_from_prims)
+        c2p_cells_kernel<true><<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(cp);
+    else
+        c2p_cells_kernel<false><<<grid1d((int64_t)G.nx * G.ny), kThreads, 0, st>>>(cp);
     launch_ghost_cc<R>(G, prims, 9, st);
 }
 
@@ -1410,10 +1430,12 @@ void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Sc
         launch_sweep2d(g, s, 0, sc.Fx, &diag->sweep[0], st);
         launch_sweep2d(g, s, 1, sc.Fy, &diag->sweep[1], st);
         launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
-        // mixed form: stage 0 solves every cell's C2P in full and keeps the
-        // roots; the later stages of the step start from them (within the
-        // step only, so a step never depends on earlier calls)
-        if (stage == 0) launch_sync_state(g, s, nullptr, diag, st, sc.mu_warm, nullptr);
+        // mixed form: stage 0 starts every cell's C2P root search from the
+        // step's input primitives (mu = 1 / (h W)) and keeps the roots; the
+        // later stages start from those (so a step depends on its input
+        // state alone)
+        if (stage == 0) launch_sync_state(g, s, nullptr, diag, st, sc.mu_warm, nullptr,
+                                            sc.mu_warm != nullptr);
         else launch_sync_state(g, s, nullptr, diag, st, nullptr, sc.mu_warm);
     }
 }

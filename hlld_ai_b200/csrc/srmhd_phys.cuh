@@ -53,6 +53,7 @@ template <> struct K<double> {
     static constexpr double mp_eps = 1e-40;
     static constexpr double safe_df = 1e-30;
     static constexpr int mu_plus_iters = 50;
+    static constexpr double warm_step = 1e-7;  // relative offset of a started C2P secant
 };
 template <> struct K<float> {
     static constexpr float tiny = 1e-30f;
@@ -62,6 +63,7 @@ template <> struct K<float> {
     static constexpr float mp_eps = 1e-30f;
     static constexpr float safe_df = 1e-30f;
     static constexpr int mu_plus_iters = 24;
+    static constexpr float warm_step = 1e-3f;  // well above FP32 round-off of the master function
 };
 
 }  // namespace hlld
@@ -466,7 +468,10 @@ __device__ __forceinline__ void kastaun_bisect(const Kastaun<T> &k, T mu_plus, C
 // c2p.py:313-363 conservative_to_primitive for one element; P gets the nine
 // primitives (B copied from C).
 // Warm start (used by the mixed-precision form only): a secant on the
-// master function from the previous root mu0 of the same cell.  It returns
+// master function from an estimate mu0 of the root -- the same cell's root
+// at the previous RK stage, the root 1 / (h W) of its primitives at the
+// start of the step, or for the HLL state of a face the mean of its two
+// sides' roots.  It returns
 // false -- and the caller runs the full bracketed solve -- unless it reaches
 // |f| < tol within eight steps at a positive root.  The master function has
 // a single root in the physical interval (0, mu+], and a start next to it
@@ -475,7 +480,7 @@ template <typename T>
 __device__ __forceinline__ bool kastaun_warm(const Kastaun<T> &k, T mu0, C2POut<T> &o) {
     const T tol = K<T>::c2p_tol;
     if (!(mu0 > T(0)) || !(mu0 < (T(1) / K<T>::tiny))) return false;
-    T x0 = mu0 * (T(1) - T(1e-7)), x1 = mu0;
+    T x0 = mu0 * (T(1) - K<T>::warm_step), x1 = mu0;
     T f0 = k.master(x0), f1 = k.master(x1);
 #pragma unroll 1
     for (int it = 0; it < 8; ++it) {
@@ -585,6 +590,7 @@ __device__ __forceinline__ void cons_to_prim_tangent(const D *C, double gamma, d
 
 template <typename T> struct Side {
     T u[NCONS], f[NCONS];
+    T mu;  // Kastaun's C2P root of the side's state, 1 / (h W)
 };
 
 // hlld.py:100-113 compute_cp_cm (flat space)
@@ -631,6 +637,7 @@ __device__ __forceinline__ void phys_side(const T *P, T gamma, Side<T> &s, T &cp
     for (int i = 0; i < 3; ++i) bs[i] = B[i] / W + vdotB * v[i] * W;
     T rho = P[P_RHO], eps = P[P_EPS];
     T h = T(1) + eps + p / rho;
+    s.mu = T(1) / (h * W);
     T v02 = cs2 + (b2 / (rho * h + b2)) * (T(1) - cs2);
     cp_cm(v02, W, v[IDIR], cp, cm);
     T d = rho * W;
@@ -1026,7 +1033,14 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         TC Ch[NCONS], Ph[NPRIM];
 #pragma unroll
         for (int k = 0; k < NCONS; ++k) Ch[k] = (TC)uH[k];
-        cons_to_prim<TC>(Ch, (TC)gamma, TC(1e-10), TC(1e-10), Ph);
+        // FP32 (the mixed form): the root search starts from the mean of the
+        // two sides' roots, next to the HLL state's own, and takes the
+        // bracketed solve only if that start does not converge; the FP64
+        // forms solve from the bracket as the reference does
+        TC mu_start = TC(0);
+        if constexpr (sizeof(TC) == sizeof(float))
+            mu_start = TC(0.5) * ((TC)ph.L.mu + (TC)ph.R.mu);
+        cons_to_prim<TC>(Ch, (TC)gamma, TC(1e-10), TC(1e-10), Ph, nullptr, mu_start);
         TC pp, cs2;
         eos_press_cs2(Ph[P_EPS], Ph[P_RHO], (TC)gamma, pp, cs2);
         TC w = lorentz_W(Ph);

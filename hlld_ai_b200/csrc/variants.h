@@ -35,7 +35,7 @@ struct Scratch2D {
                              cudaStream_t st);                                                    \
     void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,      \
                            hlld_step_diag_t *diag, cudaStream_t st, double *mu_out = nullptr,     \
-                           double *mu_warm = nullptr);                                             \
+                           double *mu_warm = nullptr, bool start_from_prims = false);             \
     void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,  \
                            double dt_host, const double *dt_dev, int scheme,                      \
                            hlld_step_diag_t *diag, cudaStream_t st);                              \

@@ -227,13 +227,26 @@ int hlld_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *st
  * physical cells written): mu_out (may be NULL) receives each cell's root;
  * mu_start (HLLD_MIXED only, may be NULL) holds a previous root of each cell
  * to start the root search from, and is updated.  hlld_rk_step_ct does the
- * same internally in the mixed form: its first stage solves every cell in
- * full and its later stages start from those roots.  (The reference
- * always solves from the bracket, c2p.py:188-236; a started search reaches
- * the same |f| < 1e-15 root, and falls back to the bracketed solve if it does
- * not within eight steps.) */
+ * same internally in the mixed form: its first stage starts from the step's
+ * input primitives (hlld_sync_state_from_prims) and its later stages start
+ * from the first stage's roots.  (The reference always solves from the
+ * bracket, c2p.py:188-236; a started search reaches the same |f| < 1e-15
+ * root, and falls back to the bracketed solve if it does not within eight
+ * steps.) */
 int hlld_sync_state_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
                           hlld_step_diag_t *diag, double *mu_out, double *mu_start, void *stream);
+
+/* hlld_sync_state (HLLD_MIXED only) whose C2P starts each physical cell's
+ * root search from the primitives the state holds on entry -- Kastaun's
+ * root is mu = 1 / (h W), h = 1 + eps + p / rho -- which the call then
+ * overwrites with the primitives of the current conserved state.  mu_out
+ * (may be NULL) receives the roots.  This is the first RK stage's sync in
+ * the mixed hlld_rk_step_ct: the primitives are the step's input, the
+ * conserved state the stage's update.  Cells whose primitives are not
+ * physical (v >= 1, rho <= 0) and starts that do not converge within eight
+ * secant steps take the bracketed solve of c2p.py:188-236. */
+int hlld_sync_state_from_prims(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
+                               hlld_step_diag_t *diag, double *mu_out, void *stream);
 
 /* Replaces src/physics/sweep.py:30-119 sweep() in the form the 2D step uses
  * it (reconstruct_prims, normal B taken from the staggered faces

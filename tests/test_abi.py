@@ -106,6 +106,19 @@ def test_scratch_size_and_argument_errors_without_gpu():
                                 None, None, None) == -1
     assert L.hlld_cons_to_prim(10, None, 5 / 3, 1e-10, 1e-10, 0, None, None, None) == -1
     assert L.hlld_error_string(-4) == b"scratch buffer too small"
+    # the C2P start from the primitives belongs to the mixed form: a NULL state
+    # and an FP64 grid are refused on the host (the non-NULL addresses of the
+    # second state are never dereferenced)
+    assert L.hlld_sync_state_from_prims(ctypes.byref(g), ctypes.byref(s), None, None, None,
+                                        None) == -1
+    fake = _lib.State2DC()
+    for k in range(6):
+        fake.cons[k] = 256
+    for k in range(9):
+        fake.prims[k] = 256
+    fake.Bxf = fake.Byf = 256
+    assert L.hlld_sync_state_from_prims(ctypes.byref(grid(precision=0)), ctypes.byref(fake), None,
+                                        None, None, None) == -3
 
 
 def test_tube_batch_argument_errors_without_gpu():

@@ -1,9 +1,9 @@
 """The step's components through the C ABI -- hlld_sweep2d, hlld_ct_update2d,
 hlld_sync_state(_roots) -- reproduce hlld_rk_step_ct bit for bit, in every
 precision.  (A host that schedules the components itself, the bench's
-per-kernel timing among them, runs exactly the production step; in the
-mixed form that includes the started C2P root solves of RK stages 2 and 3
-from the stage-1 roots of every cell.)"""
+per-kernel timing among them, runs exactly the production step.  In the
+mixed form that includes the started C2P root solves: stage 1 starts from
+the step's input primitives, stages 2 and 3 from the roots of stage 1.)"""
 import ctypes
 
 import pytest
@@ -43,10 +43,12 @@ def _component_step(stepper, st, dt, scheme, precision):
         _lib.check(L.hlld_ct_update2d(ctypes.byref(gc), ctypes.byref(s), pFx, pFy, Ez.data_ptr(),
                                       pU0, Bx0.data_ptr(), By0.data_ptr(), diag.data_ptr(), stage,
                                       nst, 0.0, dt_dev.data_ptr(), sh), "ct_update2d")
-        if mixed:
-            rc = L.hlld_sync_state_roots(ctypes.byref(gc), ctypes.byref(s), None, None,
-                                         mu.data_ptr() if stage == 0 else None,
-                                         None if stage == 0 else mu.data_ptr(), sh)
+        if mixed and stage == 0:
+            rc = L.hlld_sync_state_from_prims(ctypes.byref(gc), ctypes.byref(s), None, None,
+                                              mu.data_ptr(), sh)
+        elif mixed:
+            rc = L.hlld_sync_state_roots(ctypes.byref(gc), ctypes.byref(s), None, None, None,
+                                         mu.data_ptr(), sh)
         else:
             rc = L.hlld_sync_state(ctypes.byref(gc), ctypes.byref(s), None, None, sh)
         _lib.check(rc, "sync")
