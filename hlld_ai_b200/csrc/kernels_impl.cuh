@@ -1129,7 +1129,12 @@ __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
                     double Cd[NCONS], Pd[NPRIM];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) Cd[k] = p.U[k][base + c];
-                    cons_to_prim<double>(Cd, p.gamma, p.atmo_rho, 1e-10, Pd);
+                    // mixed form: the root search starts from the root of the
+                    // cell's primitives before the stage, which this C2P
+                    // overwrites (the 2D step's first-stage start)
+                    double mu0 = 0.0;
+                    if constexpr (sizeof(R) == sizeof(float)) mu0 = kastaun_mu_of_prims(p.P, base + c);
+                    cons_to_prim<double>(Cd, p.gamma, p.atmo_rho, 1e-10, Pd, nullptr, mu0);
 #pragma unroll
                     for (int k = 0; k < NPRIM; ++k) p.P[k][base + c] = (R)Pd[k];
                 }
