@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-fp64-arm", action="store_true",
                     help="skip timing the FP64 step and the mixed-vs-FP64 L1 check")
     ap.add_argument("--cfl", type=float, default=0.4)
+    ap.add_argument("--t-start", type=float, default=0.0,
+                    help="advance the rotor to this time (untimed) before the warm-up")
     ap.add_argument("--cpu-n", type=int, default=1024, help="grid of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -202,6 +204,11 @@ def _timed_rotor(a, precision, rp, record=True):
                                        precision=precision)
     stepper = H.Stepper2D(g, eos, bc_x=spec["bc"][0], bc_y=spec["bc"][1], flux_fn="hlld",
                           limiter="mc", precision=precision)
+    t = 0.0
+    while t < a.t_start:  # untimed: a later state of the same run
+        dt_t = stepper.compute_dt(st, a.cfl)
+        stepper.step(st, dt_t, "rk3")
+        t += float(dt_t.item())
     s = stepper._struct(st)
     gc = stepper.gc
     L = _lib.lib()
@@ -275,8 +282,12 @@ def _timed_rotor(a, precision, rp, record=True):
     clk = clocks.stop() if clocks else None
     value, ms = replicas.job_rate(rp, g.nx * g.ny * a.steps, t0.elapsed_time(t1))
     sweep_ms = [e0.elapsed_time(e1) for e0, e1 in sweep_events]
+    # share of faces without normal field (HLLE fallback, no p* solve in the
+    # mixed form) in the last timed stage's x and y sweeps
+    d = _lib.StepDiag.from_buffer_copy(diag.cpu().numpy().tobytes())
+    bn0 = [d.sweep[k].n_bn_zero / max(d.sweep[k].n_faces, 1) for k in (0, 1)]
     return dict(g=g, eos=eos, st=st, spec=spec, stepper=stepper, ms=ms, sweep_ms=sweep_ms,
-                clocks=clk, faces=(nfx + nfy) / 2.0, value=value)
+                clocks=clk, faces=(nfx + nfy) / 2.0, value=value, bn_zero_share=bn0)
 
 
 def _l1_mixed_vs_fp64(a, dev, steps):
@@ -469,8 +480,11 @@ def run_ours(a):
             "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "n": a.n, "precision": a.precision,
+                       "t_start": a.t_start,
                        "parallelism": f"replicas x{world}", "cfl": a.cfl,
-                       "l2": "inputs exceed L2 (state >1 GB at 2048^2), no flush"},
+                       "l2": "inputs exceed L2 (state >1 GB at 2048^2), no flush",
+                       "bn_zero_face_share": {"x": main["bn_zero_share"][0],
+                                              "y": main["bn_zero_share"][1]}},
             "fp64": fp64_arm,
             "adjoint": adj,
             "e2e": e2e,

@@ -1069,6 +1069,26 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
     }
     const T BnL = ph.L.u[Bn], BnR = ph.R.u[Bn];
     bool bn_zero = (fabs(BnL) < T(1e-14)) && (fabs(BnR) < T(1e-14));
+    // A face without normal field always takes the HLLE fallback
+    // (hlld.py:1512-1531): its flux, state and p* output do not depend on the
+    // p* solve, which feeds only the solver counters.  The mixed form (FP32
+    // HLL-state C2P) skips the solve there and marks the face err = -1, so
+    // its counters cover the faces it solves; the FP64 forms solve every face
+    // as the reference does.
+    if constexpr (!IFT && sizeof(TC) == sizeof(float)) {
+        if (bn_zero) {
+#pragma unroll
+            for (int k = 0; k < NCONS; ++k) {
+                o.F[k] = fH[k];
+                if (want_u) o.U[k] = uH[k];
+            }
+            o.pstar = (T)(-fabs(p_hll) - TP(1e-10));
+            o.err = -1;
+            o.iters = 0;
+            o.flags = RF_BN_ZERO | RF_FAILED;
+            return;
+        }
+    }
 
     // R vectors on the energy-form state (hlld.py:337-360, :401-428)
     HlldR<TP> C;
