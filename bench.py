@@ -328,9 +328,9 @@ _SWEEP_DRAM_BYTES_PER_FACE_MIXED = (136.3e6 + 133.7e6) / 2 / 2373140
 
 
 # DRAM bytes (read + write) of one mixed-precision tubes_kernel launch
-# measured by ncu (2048 seeded tubes, chunk 0.0005: 5.88 + 9.84 GB over
+# measured by ncu (2048 seeded tubes, chunk 0.0005: 8.05 + 11.53 GB over
 # 2.129e7 cell-updates), per cell-update; a launch is scaled by its updates
-_TUBES_DRAM_BYTES_PER_UPDATE_MIXED = (5.876e9 + 9.840e9) / 2.129e7
+_TUBES_DRAM_BYTES_PER_UPDATE_MIXED = (8.053e9 + 11.526e9) / 2.129e7
 
 
 def _sweep_traffic(a):
