@@ -63,7 +63,11 @@ enum hlld_bc { HLLD_BC_OUTFLOW = 0, HLLD_BC_PERIODIC = 1 };
 #define HLLD_RF_FAILED 4u
 
 /* Device-resident counters of one flux sweep: the numbers the reference
- * keeps in hlld.LAST_DIAG (src/physics/hlld.py:1516-1529). */
+ * keeps in hlld.LAST_DIAG (src/physics/hlld.py:1516-1529).  In HLLD_MIXED
+ * the sweep does not solve p* on faces with B_n = 0, whose HLLE fallback
+ * result does not depend on it.  Those faces count in n_faces, n_bn_zero
+ * and n_failed only, so n_not_converged, n_wave_order_bad, iters_sum_conv,
+ * n_conv and max_iters cover the faces that were solved. */
 typedef struct {
     unsigned long long n_faces;
     unsigned long long n_not_converged;
