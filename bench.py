@@ -322,9 +322,9 @@ def _l1_mixed_vs_fp64(a, dev, steps):
 
 
 # DRAM bytes (read + write) of one mixed-precision sweep launch measured by
-# ncu on the rotor at 1536^2 (x: 95.0 + 41.3 MB, y: 95.0 + 38.7 MB over
+# ncu on the rotor at 1536^2 (x: 95.0 + 79.4 MB, y: 95.5 + 54.2 MB over
 # 2,373,140 faces), per face; the 2048^2 launch is scaled by its faces
-_SWEEP_DRAM_BYTES_PER_FACE_MIXED = (136.3e6 + 133.7e6) / 2 / 2373140
+_SWEEP_DRAM_BYTES_PER_FACE_MIXED = (174.3e6 + 149.7e6) / 2 / 2373140
 
 
 # DRAM bytes (read + write) of one mixed-precision tubes_kernel launch
