@@ -101,6 +101,24 @@ template <typename T> __device__ __forceinline__ T sdiv(T num, T den) {
     return num / den;
 }
 
+// Reciprocal by Newton's method on f(y) = 1/y - d, whose step
+// y <- y + y (1 - d y) squares the relative error: the hardware's
+// approximate reciprocal as the seed and three steps, which leave an error of
+// a few ulp.  Used by the mixed form's FP64 p* solve (HLLD_NR_RCP), where the
+// secant's 1e-10 tolerance is far above it.  d must be a normal double; the
+// callers clamp it to |d| >= 1e-300.
+__device__ __forceinline__ double nr_rcp(double d) {
+#if defined(__CUDA_ARCH__)
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) y = fma(y, fma(-d, y, 1.0), y);
+    return y;
+#else
+    return 1.0 / d;
+#endif
+}
+
 // Division by a denominator shared by several quotients.  The exact form
 // (HLLD_EXACT_ARITH) divides each numerator as the reference does; the fast
 // forms multiply by one reciprocal of the same safe denominator (the _sdiv
@@ -116,6 +134,9 @@ template <typename T> struct SharedDen {
         }
 #if HLLD_EXACT_ARITH
         den = d;
+#elif defined(HLLD_NR_RCP)
+        if constexpr (sizeof(T) == sizeof(double)) den = nr_rcp(d);
+        else den = T(1) / d;
 #else
         den = T(1) / d;
 #endif

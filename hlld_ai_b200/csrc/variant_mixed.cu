@@ -3,6 +3,7 @@
 // divergence; FP64 HLLD p* bracket and iteration, HLLD star states, cell C2P
 // and RK accumulation of the conserved state and the staggered field.
 #define HLLD_NS v_mixed
+#define HLLD_NR_RCP 1  // Newton reciprocal for the FP64 p* solve's shared denominators
 #define HLLD_REAL float
 #ifndef HLLD_BRACKET_REAL
 #define HLLD_BRACKET_REAL float
