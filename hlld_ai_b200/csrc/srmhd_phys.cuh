@@ -119,6 +119,19 @@ __device__ __forceinline__ double nr_rcp(double d) {
 #endif
 }
 
+// 1 / x for the Kastaun master function: the Newton reciprocal in the mixed
+// form's FP64 cell C2P, a division everywhere else (the FP64 forms keep the
+// reference's quotients).
+#if defined(HLLD_NR_RCP)
+template <typename T> constexpr bool kNewtonRcp = sizeof(T) == sizeof(double);
+#else
+template <typename T> constexpr bool kNewtonRcp = false;
+#endif
+template <typename T> __device__ __forceinline__ T rcp_c2p(T x) {
+    if constexpr (kNewtonRcp<T>) return nr_rcp(x);
+    else return T(1) / x;
+}
+
 // Division by a denominator shared by several quotients.  The exact form
 // (HLLD_EXACT_ARITH) divides each numerator as the reference does; the fast
 // forms multiply by one reciprocal of the same safe denominator (the _sdiv
@@ -230,7 +243,7 @@ template <typename T> struct Kastaun {
         gamma = g;
     }
     // c2p.py:110-127
-    __device__ __forceinline__ T chi(T mu) const { return T(1) / (T(1) + mu * BtNorm2); }
+    __device__ __forceinline__ T chi(T mu) const { return rcp_c2p(T(1) + mu * BtNorm2); }
     __device__ __forceinline__ T rbar2(T mu) const {
         T c = chi(mu);
         return rNorm2 * (c * c) + mu * c * (T(1) + c) * (B_dot_r * B_dot_r);
@@ -247,15 +260,18 @@ template <typename T> struct Kastaun {
         T qb = qbar(mu);
         T rb2 = rbar2(mu);
         T vhat2 = tmin((mu * mu) * rb2, v02);
-        T What = T(1) / sqrt(clamp_lo(T(1) - vhat2, T(1e-10)));
-        T rhohat0 = D / What;
+        const T sW = sqrt(clamp_lo(T(1) - vhat2, T(1e-10)));  // 1 / What
+        T What = rcp_c2p(sW);
+        T rhohat0 = kNewtonRcp<T> ? D * sW : D / What;
         T rhohat = tmin(tmax(rhohat0, T(1e-12)), T(1e15));
-        T epshat0 = What * (qb - mu * rb2) + vhat2 * (What * What) / (T(1) + What);
+        T epshat0 = What * (qb - mu * rb2) + (kNewtonRcp<T> ? vhat2 * (What * What) * rcp_c2p(T(1) + What)
+                                                            : vhat2 * (What * What) / (T(1) + What));
         T epshat = tmin(tmax(epshat0, T(0)), T(1e5));
         T phat = eos_press(epshat, rhohat, gamma);
-        T ahat = phat / (rhohat * (T(1) + epshat) + K<T>::tiny);
+        T ahat = kNewtonRcp<T> ? phat * rcp_c2p(rhohat * (T(1) + epshat) + K<T>::tiny)
+                               : phat / (rhohat * (T(1) + epshat) + K<T>::tiny);
         T h_eff = (T(1) + ahat) * (T(1) + epshat);
-        T nu_A = h_eff / What;
+        T nu_A = kNewtonRcp<T> ? h_eff * sW : h_eff / What;
         T nu_B = (T(1) + ahat) * (T(1) + qb - mu * rb2);
         T nu = tmax(nu_A, nu_B);
         if (rho_o) *rho_o = rhohat;
