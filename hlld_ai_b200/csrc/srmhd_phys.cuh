@@ -104,8 +104,8 @@ template <typename T> __device__ __forceinline__ T sdiv(T num, T den) {
 // Reciprocal by Newton's method on f(y) = 1/y - d, whose step
 // y <- y + y (1 - d y) squares the relative error: the hardware's
 // approximate reciprocal as the seed and three steps, which leave an error of
-// a few ulp.  Used by the mixed form's FP64 p* solve (HLLD_NR_RCP), where the
-// secant's 1e-10 tolerance is far above it.  d must be a normal double; the
+// a few ulp.  Used by the mixed form's FP64 p* solve and cell C2P
+// (HLLD_NR_RCP), whose tolerances are far above it.  d must be a normal double; the
 // callers clamp it to |d| >= 1e-300.
 __device__ __forceinline__ double nr_rcp(double d) {
 #if defined(__CUDA_ARCH__)

@@ -1,7 +1,7 @@
 """The mixed form's Newton reciprocal against CUDA's division.
 
-The mixed form's FP64 p* solve multiplies by reciprocals of its shared
-denominators, computed by Newton's method on f(y) = 1/y - d from the
+The mixed form's FP64 p* solve and cell C2P multiply by reciprocals,
+computed by Newton's method on f(y) = 1/y - d from the
 hardware's approximate reciprocal (``nr_rcp`` in
 hlld_ai_b200/csrc/srmhd_phys.cuh).  ``tests/host/nr_rcp_check.cu`` runs it
 on a million doubles of both signs with exponents over [1e-300, 1e300] and
