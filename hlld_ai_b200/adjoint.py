@@ -11,7 +11,7 @@ time step fixed and every discrete decision frozen at its forward outcome
 (limiter branches, HLLD region and fallback, CT upwind signs); the HLLD p*
 and the Kastaun C2P root are differentiated by the implicit-function
 theorem.  The reference has no adjoint; its gradients would come from torch
-autograd through ``src/physics/driver2d.py:420-448`` rk_step_ct, which the
+autograd through ``src/physics/driver2d.py:221-249`` rk_step_ct, which the
 same step sequence reproduces.
 
 ``RKSteps`` wraps a run in a ``torch.autograd.Function`` over the conserved

@@ -13,7 +13,7 @@
 // hlld.py:586-602) and the Kastaun root mu of the C2P master function
 // (c2p.py:129-158), both in dual arithmetic from the solved root.
 //
-// Reverse of stage s (driver2d.py:382-391 combine + sync):
+// Reverse of stage s (driver2d.py:183-192 combine + sync):
 //   a. primitive ghost fill (fold the ghost lambdas onto their sources)
 //   b. C2P of the physical cells (reverse mode at the recorded root, IFT on
 //      mu: c2p_vjp.cuh)

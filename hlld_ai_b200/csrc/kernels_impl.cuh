@@ -13,8 +13,8 @@
 //   ct_update_kernel      flux divergence + CT face update + RK combine
 //                         (sweep.py:122-135, ct.py:180-185, state.py:77-103)
 //   ghost_kernel          separable ghost fill (grid.py:93-143, :229-255)
-//   c2p_cells_kernel      cell-centred B + C2P of physical cells (driver2d.py:395-417)
-//   speed_kernel/dt_kernel compute_dt_2d (driver2d.py:251-281)
+//   c2p_cells_kernel      cell-centred B + C2P of physical cells (driver2d.py:196-218)
+//   speed_kernel/dt_kernel compute_dt_2d (driver2d.py:52-82)
 #pragma once
 
 #ifndef HLLD_NS
@@ -770,7 +770,7 @@ struct SpeedParams {
     unsigned long long *out;  // [2]
 };
 
-// max(|v_d| + c_f) over the physical cells (driver2d.py:260-279), in double
+// max(|v_d| + c_f) over the physical cells (driver2d.py:61-80), in double
 __global__ void __launch_bounds__(kThreads) speed_kernel(const SpeedParams p) {
     const Grid &g = p.g;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -822,7 +822,7 @@ __constant__ double kRK2d[2][3] = {{1.0, 0.0, 1.0}, {0.5, 0.5, 0.5}};
 
 // ── batched 1D tubes (one persistent launch) ─────────────────────────────
 //
-// Each tube is driver2d.py:309-355 rk_step on a ny = 1 grid (whose y sweep
+// Each tube is driver2d.py:110-156 rk_step on a ny = 1 grid (whose y sweep
 // contributes exactly zero), advanced to tend with its own dt
 // (driver.py:77-127 compute_dt).  A CTA takes whole tubes from an atomic
 // counter (in the caller's order, e.g. longest first) and time-steps each

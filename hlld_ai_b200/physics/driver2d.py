@@ -2,7 +2,7 @@
 
 ``rk_step_ct``, ``sync_state``, ``compute_dt_2d``, ``prims_to_cons_2d`` and
 ``cons_to_prims_2d`` keep the reference signatures and semantics
-(``driver2d.py:251-448``); the work is done by libhlld_b200.so.  One RK
+(``driver2d.py:52-249``); the work is done by libhlld_b200.so.  One RK
 step is ``scheme`` stages of five launches each -- x sweep, y sweep (fused
 reconstruction + Riemann solve), corner EMF, update (flux divergence + CT +
 RK combine), sync (ghosts, C2P, ghosts) -- enqueued by ``hlld_rk_step_ct``.
@@ -143,7 +143,7 @@ class Stepper2D:
 
 class StepDiag(Mapping):
     """``{"x": {"diag": ...}, "y": {"diag": ...}, "c2p": ...}`` of the last
-    step (driver2d.py:441-448); the device counters are copied to the host
+    step (driver2d.py:242-249); the device counters are copied to the host
     on first access."""
 
     def __init__(self, raw: torch.Tensor):
@@ -194,7 +194,7 @@ def _opts(bc_x, bc_y, flux_fn, limiter, vel_var, emf_mode, upwind, atmo_rho, pre
 def rk_step_ct(state, grid, eos, dt, *, scheme="rk3", bc_x="outflow", bc_y="outflow",
                flux_fn="hlld", limiter="mc", vel_var="Wv", emf_mode="solver", upwind=True,
                atmo_rho=1e-10, recorder=None, precision="fp64"):
-    """driver2d.py:420-448.  Returns a new State2D (the input is left as it
+    """driver2d.py:221-249.  Returns a new State2D (the input is left as it
     was, as in the reference) and the last stage's sweep diagnostics."""
     if recorder is not None:
         raise NotImplementedError("interface-state recording is not part of the B200 step")
@@ -210,7 +210,7 @@ def rk_step_ct(state, grid, eos, dt, *, scheme="rk3", bc_x="outflow", bc_y="outf
 
 def sync_state(state, grid, eos, bc_x="outflow", bc_y="outflow", atmo_rho=1e-10,
                return_status=False, precision="fp64", limiter="mc"):
-    """driver2d.py:395-417, in place; returns the state (and C2P status)."""
+    """driver2d.py:196-218, in place; returns the state (and C2P status)."""
     st = stepper_for(grid, eos, **_opts(bc_x, bc_y, "hlld", limiter, "Wv", "solver", True,
                                         atmo_rho, precision))
     status = (torch.zeros(grid.nxt, grid.nyt, dtype=torch.uint8, device=st.device)
@@ -228,7 +228,7 @@ def sync_state(state, grid, eos, bc_x="outflow", bc_y="outflow", atmo_rho=1e-10,
 
 
 def compute_dt_2d(prims, grid, eos, cfl, speed_of_light=False, precision="fp64") -> float:
-    """driver2d.py:251-281 (one device->host read, as the reference's float())."""
+    """driver2d.py:52-82 (one device->host read, as the reference's float())."""
     if speed_of_light:
         one = torch.ones((), dtype=torch.float64)
         return float(cfl / (one / grid.dx + one / grid.dy))
@@ -242,12 +242,12 @@ def compute_dt_2d(prims, grid, eos, cfl, speed_of_light=False, precision="fp64")
 
 
 def prims_to_cons_2d(prims: dict, grid, precision="fp64") -> dict:
-    """driver2d.py:296-297"""
+    """driver2d.py:97-98"""
     return unflat(primitive_to_conserved(flat(prims), precision), grid.shape)
 
 
 def cons_to_prims_2d(cons: dict, grid, eos, atmo_rho: float = 1e-10, return_status=False):
-    """driver2d.py:284-293"""
+    """driver2d.py:85-94"""
     out = conservative_to_primitive(flat(cons), eos, atmo_rho=atmo_rho, return_status=return_status)
     if return_status:
         prims, status = out

@@ -31,7 +31,7 @@ SOLVERS = ("hlld", "hlle", "hllc")
 
 
 def _bs(grid, eos):
-    """Beckwith & Stone's Orszag-Tang (initial_data2d.py:522-536)."""
+    """Beckwith & Stone's Orszag-Tang (initial_data2d.py:256-270)."""
     import math
     return orszag_tang(grid, eos, v_max=0.5 * math.sqrt(2.0))
 

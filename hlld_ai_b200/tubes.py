@@ -2,7 +2,7 @@
 
 The B200 form of ``src/physics/tube_seed.py:93-144`` run_tubes for
 thousands of tubes of uneven length: every tube runs the reference's no-CT
-step (``driver2d.py:309-355`` rk_step on a ny = 1 grid, WENO5-Z / PLM,
+step (``driver2d.py:110-156`` rk_step on a ny = 1 grid, WENO5-Z / PLM,
 HLLD / HLLE, SSP-RK3) with its OWN CFL time step (``driver.py:77-127``) to
 ``tend``.  All tubes advance in a single launch of ``hlld_tubes_run``: each
 CTA takes whole tubes, longest first, from a device work counter.  The

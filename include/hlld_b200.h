@@ -81,7 +81,7 @@ typedef struct {
 } hlld_flux_diag_t;
 
 /* Device-resident counters of one RK step (last stage's sweeps, as the
- * reference's rk_step_ct returns, src/physics/driver2d.py:441-448). */
+ * reference's rk_step_ct returns, src/physics/driver2d.py:242-249). */
 typedef struct {
     hlld_flux_diag_t sweep[2];
     unsigned long long c2p_not_converged;
@@ -126,7 +126,7 @@ typedef struct {
 
 /* How each tube of a batch is stepped (hlld_tubes_t.flavor). */
 enum hlld_tube_flavor {
-    /* src/physics/driver2d.py:309-355 rk_step on a ny = 1 grid: W v
+    /* src/physics/driver2d.py:110-156 rk_step on a ny = 1 grid: W v
      * reconstruction with the PCM positivity fallback, SSP-RK2/3 per
      * `scheme`, dt = compute_dt (driver.py:77-127) with the fast speed,
      * stepping while t < tend - 1e-14 */
@@ -198,9 +198,9 @@ int hlld_riemann_faces(int64_t n, const void *const *sL, const void *const *sR, 
  * EMF, the RK stage-0 copy). */
 int hlld_step2d_scratch_bytes(const hlld_grid2d_t *g, size_t *bytes);
 
-/* Replaces src/physics/driver2d.py:420-448 rk_step_ct (with ct_stage
- * :361-392, sweep.py:30-135, ct.py:44-199, state.py:77-103 combine and
- * sync_state :395-417): one SSP-RK2 (scheme 2) or RK3 (scheme 3) step with
+/* Replaces src/physics/driver2d.py:221-249 rk_step_ct (with ct_stage
+ * :162-193, sweep.py:30-135, ct.py:44-199, state.py:77-103 combine and
+ * sync_state :196-218): one SSP-RK2 (scheme 2) or RK3 (scheme 3) step with
  * constrained transport, in place on s.  dt is read from dt_dev when it is
  * not NULL (device scalar, lets the step be graph-captured), else dt_host.
  * diag (device, may be NULL) is zeroed and filled. */
@@ -221,7 +221,7 @@ int hlld_rk_step_ct_static(const hlld_grid2d_t *g, const hlld_state2d_t *s, doub
                            const double *dt_dev, int scheme, hlld_step_diag_t *diag,
                            void *stream);
 
-/* Replaces src/physics/driver2d.py:395-417 sync_state: face BCs, cell BCs,
+/* Replaces src/physics/driver2d.py:196-218 sync_state: face BCs, cell BCs,
  * cell-centred B, C2P of the physical cells, primitive BCs, in place.
  * status (nxt*nyt, may be NULL) gets HLLD_ST_* bits of the physical cells. */
 int hlld_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
@@ -263,7 +263,7 @@ int hlld_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void
                  hlld_flux_diag_t *diag, void *stream);
 
 /* Replaces the rest of ct_stage + combine for RK stage `stage` (0-based) of
- * `scheme` (src/physics/driver2d.py:382-391, :440-445; ct.py:57-185;
+ * `scheme` (src/physics/driver2d.py:183-192, :241-246; ct.py:57-185;
  * sweep.py:122-135; state.py:77-103): corner EMF, flux divergence, CT face
  * update and the SSP-RK combine, in place on s.  Fx, Fy: the two sweeps'
  * outputs; Ez: (nxt+1)(nyt+1) work array; U0 (6 cell arrays), Bx0, By0: the
@@ -275,7 +275,7 @@ int hlld_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *cons
                      const double *dt_dev, void *stream);
 
 /* Replaces src/physics/tube_seed.py:93-144 run_tubes for the batched-tube
- * workload, with a dt per tube: every tube runs src/physics/driver2d.py:309-355
+ * workload, with a dt per tube: every tube runs src/physics/driver2d.py:110-156
  * rk_step on a ny = 1 grid (x sweep only -- the y sweep of a ny = 1 grid
  * contributes exactly zero), dt from src/physics/driver.py:77-127
  * compute_dt each step, until tend or max_steps (flavor HLLD_TUBE_RK_STEP),
@@ -322,7 +322,7 @@ int hlld_adjoint_scratch_bytes(const hlld_grid2d_t *g, size_t *bytes);
 
 /* Discrete adjoint of one hlld_rk_step_ct step.  No counterpart in the
  * reference, whose gradients would come from torch autograd through
- * src/physics/driver2d.py:420-448 rk_step_ct; this is that step's
+ * src/physics/driver2d.py:221-249 rk_step_ct; this is that step's
  * transpose with its dt held fixed.  s_in is the step's input state and
  * s_out the output the forward step made from it with dt.  lam (device
  * arrays shaped like a state: cons[6], Bxf, Byf, prims[9], double) holds
@@ -339,7 +339,7 @@ int hlld_adjoint_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s_in,
                             const hlld_state2d_t *lam, void *scratch, size_t scratch_bytes,
                             void *stream);
 
-/* Replaces src/physics/driver2d.py:251-281 compute_dt_2d: writes
+/* Replaces src/physics/driver2d.py:52-82 compute_dt_2d: writes
  * dt = cfl / (max(|vx|+cf)/dx + max(|vy|+cf)/dy) to dt_dev (device double);
  * work (device, >= 2 unsigned long long) holds the running maxima. */
 int hlld_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,

@@ -195,7 +195,7 @@ def _state_ptrs(state: dict):
 
 
 def sync_state(g: Grid2DSpec, state: dict) -> np.ndarray:
-    """``driver2d.py:395-417`` in place on numpy arrays; returns C2P status."""
+    """``driver2d.py:196-218`` in place on numpy arrays; returns C2P status."""
     cons, prim = _state_ptrs(state)
     st = np.zeros(state["cons"]["D"].shape, dtype=np.uint8)
     gc = g.c()
@@ -204,7 +204,7 @@ def sync_state(g: Grid2DSpec, state: dict) -> np.ndarray:
 
 
 def rk_step_ct(g: Grid2DSpec, state: dict, dt: float, scheme: str = "rk3") -> dict:
-    """``driver2d.py:420-448`` in place; returns the last stage's sweep diag."""
+    """``driver2d.py:221-249`` in place; returns the last stage's sweep diag."""
     cons, prim = _state_ptrs(state)
     d = _Diag()
     gc = g.c()
@@ -217,7 +217,7 @@ def rk_step_ct(g: Grid2DSpec, state: dict, dt: float, scheme: str = "rk3") -> di
 
 
 def compute_dt_2d(g: Grid2DSpec, prims: dict, cfl: float) -> float:
-    """``driver2d.py:251-281``."""
+    """``driver2d.py:52-82``."""
     P = _ptrs([_f64(prims[k]) for k in PRIM_KEYS])
     gc = g.c()
     return float(lib().orc_compute_dt_2d(ctypes.byref(gc), P, ctypes.c_double(cfl)))
@@ -237,7 +237,7 @@ def rk2_step_1d(cons: dict, prims: dict, ncells: int, ng: int, dx: float, dt: fl
 def tube_run(prims: dict, L: int, ng: int, dx: float, cfl: float, tend: float, limiter: str,
              solver: str, gamma: float, scheme: str = "rk3", max_steps: int = 1 << 30,
              atmo_rho: float = 1e-10):
-    """One 1D tube to tend (driver2d.py:309-355 on a ny = 1 grid), in place
+    """One 1D tube to tend (driver2d.py:110-156 on a ny = 1 grid), in place
     on 9 primitive arrays of L + 2 ng cells; returns (t, steps)."""
     P = _ptrs([prims[k] for k in PRIM_KEYS])
     t = ctypes.c_double(0.0)

@@ -59,16 +59,16 @@ static inline double sdiv(double num, double den) {
 
 /* ── EOS: hybrid_eos(K=0, gamma, gamma_th=gamma) (eos.py:32-76) ────────── */
 
-/* eos.py:47-54 press__eps_rho with press_cold = eps_cold = 0 */
+/* eos.py:32-39 press__eps_rho with press_cold = eps_cold = 0 */
 static inline double eos_press(double eps, double rho, double gamma) {
     double e = tmax(eps, 0.0);
     return 0.0 + (e - 0.0) * rho * (gamma - 1.0);
 }
-/* eos.py:56-61 eps__press_rho */
+/* eos.py:41-46 eps__press_rho */
 static inline double eos_eps(double press, double rho, double gamma) {
     return 0.0 + (press - 0.0) / (rho * (gamma - 1.0));
 }
-/* eos.py:80-91 press_and_cs2 (not cold: gamma_th = gamma != 1) */
+/* eos.py:65-76 press_and_cs2 (not cold: gamma_th = gamma != 1) */
 static inline void eos_press_cs2(double eps, double rho, double gamma, double *p, double *cs2) {
     double press = eos_press(eps, rho, gamma);
     double h = 1.0 + eps + press / rho;
@@ -1396,7 +1396,7 @@ int orc_rk_step_ct(const orc_grid2d *g, double dt, int scheme, double *const *co
     int64_t ncr = (int64_t)(nxt + 1) * (nyt + 1);
     int nst = scheme;
     const double(*tab)[3] = scheme == 3 ? RK3 : RK2;
-    /* S0 = clone (driver2d.py:434-436) */
+    /* S0 = clone (driver2d.py:235-237) */
     double *U0[6], *Fx[ORC_NCONS], *Fy[ORC_NCONS];
     for (int k = 0; k < 6; ++k) {
         U0[k] = (double *)malloc(sizeof(double) * (size_t)nc);
@@ -1421,7 +1421,7 @@ int orc_rk_step_ct(const orc_grid2d *g, double dt, int scheme, double *const *co
 
     for (int st = 0; st < nst; ++st) {
         double a = tab[st][0], b = tab[st][1], c = tab[st][2];
-        /* ct_stage (driver2d.py:361-392) */
+        /* ct_stage (driver2d.py:162-193) */
         cell_centred_B(nxt, nyt, Bxf, Byf, Bcx, Bcy);
         for (int k = 0; k < ORC_NPRIM; ++k) memcpy(pw[k], prim[k], sizeof(double) * (size_t)nc);
         memcpy(pw[ORC_PBX], Bcx, sizeof(double) * (size_t)nc);
@@ -1601,7 +1601,7 @@ void orc_rk2_step_1d(int ncells, int ng, double dx, double dt, int limiter, int 
     for (int k = 0; k < ORC_NPRIM; ++k) free(p1[k]);
 }
 
-/* ── batched-tube workload: one 1D tube (driver2d.py:309-355 on ny = 1) ─ */
+/* ── batched-tube workload: one 1D tube (driver2d.py:110-156 on ny = 1) ─ */
 
 /* driver.py:77-127 compute_dt with speed_of_light = False; `(cfl*dx) /
  * tensor` is torch's reciprocal(tensor) * (cfl*dx) */

@@ -112,19 +112,19 @@ typedef struct {
     double fd_max[2]; /* max |F_D| of each sweep (ct.py:114) */
 } orc_step_diag;
 
-/* driver2d.py:395-417 sync_state: face BC, cell BC, cell-centred B, C2P,
+/* driver2d.py:196-218 sync_state: face BC, cell BC, cell-centred B, C2P,
  * primitive BC.  cons: 6 arrays D, Sx, Sy, Sz, tau, Bz (state.py:41).
  * prim: 9 arrays.  status (nxt*nyt) may be NULL. */
 void orc_sync_state(const orc_grid2d *g, double *const *cons, double *Bxf, double *Byf,
                     double *const *prim, uint8_t *status);
 
-/* driver2d.py:420-448 rk_step_ct: one SSP-RK2/3 step with CT; the state
+/* driver2d.py:221-249 rk_step_ct: one SSP-RK2/3 step with CT; the state
  * (cons, faces, prims) is updated in place.  diag may be NULL (it reports
  * the last stage's sweeps, as the reference's returned diag does). */
 int orc_rk_step_ct(const orc_grid2d *g, double dt, int scheme, double *const *cons,
                    double *Bxf, double *Byf, double *const *prim, orc_step_diag *diag);
 
-/* driver2d.py:251-281 compute_dt_2d */
+/* driver2d.py:52-82 compute_dt_2d */
 double orc_compute_dt_2d(const orc_grid2d *g, const double *const *prim, double cfl);
 
 /* ct.py:119-177 corner_emf on (n0, n1) cells; Ez is (n0+1, n1+1) */
@@ -137,7 +137,7 @@ void orc_corner_emf(int n0, int n1, const double *Ec, const double *Efx, const d
 void orc_rk2_step_1d(int ncells, int ng, double dx, double dt, int limiter, int solver,
                      double gamma, double atmo_rho, double *const *cons, double *const *prim);
 
-/* One 1D tube run to tend (the batched-tube workload): driver2d.py:309-355
+/* One 1D tube run to tend (the batched-tube workload): driver2d.py:110-156
  * rk_step (no CT) on a ny = 1 grid, whose y sweep contributes exactly zero,
  * so only the x sweep is formed: reconstruct_prims of all eight work
  * variables (W v), flux_fn with idir 0, F[Bx] = 0, all eight conserved

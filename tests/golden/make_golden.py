@@ -405,7 +405,9 @@ def make_emf_hll(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_CHECKOUT [hllc|emf_hll]")
+    root = sys.argv[1]
     if len(sys.argv) > 2 and sys.argv[2] == "hllc":
         make_hllc(root)
     elif len(sys.argv) > 2 and sys.argv[2] == "emf_hll":

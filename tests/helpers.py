@@ -10,7 +10,7 @@ PRIM_KEYS = ("rho", "vx", "vy", "vz", "p", "eps", "Bx", "By", "Bz")
 
 
 def ideal_eps(p, rho, gamma):
-    """eps from p for hybrid_eos(K=0, gamma, gamma_th=gamma) (eos.py:56-61 order)."""
+    """eps from p for hybrid_eos(K=0, gamma, gamma_th=gamma) (eos.py:41-46 order)."""
     return 0.0 + (p - 0.0) / (rho * (gamma - 1.0))
 
 
