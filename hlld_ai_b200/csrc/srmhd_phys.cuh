@@ -105,10 +105,14 @@ template <typename T> __device__ __forceinline__ T sdiv(T num, T den) {
 // y <- y + y (1 - d y) squares the relative error: the hardware's
 // approximate reciprocal as the seed and three steps, which leave an error of
 // a few ulp.  Used by the mixed form's FP64 p* solve and cell C2P
-// (HLLD_NR_RCP), whose tolerances are far above it.  d must be a normal double; the
-// callers clamp it to |d| >= 1e-300.
+// (HLLD_NR_RCP), whose tolerances are far above it.  Outside 2^-1000 <= |d|
+// < 2^1000 (zero, subnormals, where the seed's flush-to-zero would give 0 or
+// inf, huge values whose reciprocal is subnormal, inf and NaN) it divides, so
+// that every input gets the quotient 1.0 / d would give.
 __device__ __forceinline__ double nr_rcp(double d) {
 #if defined(__CUDA_ARCH__)
+    const double a = fabs(d);
+    if (!(a < 0x1p1000 && a >= 0x1p-1000)) return 1.0 / d;
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
 #pragma unroll
@@ -723,11 +727,23 @@ __device__ __forceinline__ void srmhd_fluxes(const T *PL, const T *PR, T gamma, 
     ph.cmin = cmin;
 }
 
-// hlld.py:161-168
+// hlld.py:161-168.  In FP32 (the mixed form) the same average is written as
+// the left value plus a correction built from the two sides' differences.
+// The reference's weighted sum rounds an O(1) flux (the momentum flux
+// carries the total pressure) to within a few ulp that depend on the bits
+// of cx and cm, so neighbouring faces of a nearly uniform state get fluxes
+// that differ by FP32 ulps, and their divergence seeds velocity noise of
+// ~1e-8 everywhere the stencil has reached.  The difference form is exact
+// when the two sides agree and errs no more than the differences
+// themselves, so a state without signal stays without one, as in FP64.
 template <typename T> __device__ __forceinline__ T hf(T fL, T fR, T uL, T uR, T cm, T cx) {
+    if constexpr (sizeof(T) == sizeof(float))
+        return fL + cm * ((fR - fL) - cx * (uR - uL)) / (cx + cm);
     return (cx * fL + cm * fR - cx * cm * (uR - uL)) / (cx + cm);
 }
 template <typename T> __device__ __forceinline__ T hu(T fL, T fR, T uL, T uR, T cm, T cx) {
+    if constexpr (sizeof(T) == sizeof(float))
+        return uL + (cx * (uR - uL) - (fR - fL)) / (cx + cm);
     return (cx * uR + cm * uL + fL - fR) / (cx + cm);
 }
 
@@ -1048,8 +1064,10 @@ template <typename TP> __device__ __forceinline__ TP hlld_ift_root(const HlldR<T
 // p* iteration; the fast and exact forms use double for all three.
 // IFT = true is the tangent form (T = TP = Dual): given[0] is the face's
 // solved p* and given[1] != 0 its fallback decision, both from the value
-// computation; the bracket and the secant are skipped.
-template <int IDIR, typename T, typename TC = T, typename TP = T, bool IFT = false>
+// computation; the bracket and the secant are skipped.  SKIP_BN0: no p*
+// solve on faces without normal field (see below).
+template <int IDIR, typename T, typename TC = T, typename TP = T, bool IFT = false,
+          bool SKIP_BN0 = (sizeof(TC) == sizeof(float))>
 __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, bool want_u,
                                           FaceOut<T> &o, const double *given = nullptr) {
     constexpr int i = IDIR, t1 = (IDIR + 1) % 3, t2 = (IDIR + 2) % 3;
@@ -1108,11 +1126,12 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
     bool bn_zero = (fabs(BnL) < T(1e-14)) && (fabs(BnR) < T(1e-14));
     // A face without normal field always takes the HLLE fallback
     // (hlld.py:1512-1531): its flux, state and p* output do not depend on the
-    // p* solve, which feeds only the solver counters.  The mixed form (FP32
-    // HLL-state C2P) skips the solve there and marks the face err = -1, so
-    // its counters cover the faces it solves; the FP64 forms solve every face
-    // as the reference does.
-    if constexpr (!IFT && sizeof(TC) == sizeof(float)) {
+    // p* solve, which feeds only the solver counters.  With SKIP_BN0 (the 2D
+    // sweeps and the tube kernel of every form but the exact one) the solve
+    // is skipped there and the face is marked err = -1, so the counters
+    // cover the faces that were solved; the exact form and the per-face
+    // plugin solve every face as the reference does.
+    if constexpr (!IFT && SKIP_BN0) {
         if (bn_zero) {
 #pragma unroll
             for (int k = 0; k < NCONS; ++k) {
