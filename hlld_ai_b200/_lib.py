@@ -14,8 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("HLLD_B200_LIB") or os.path.join(HERE, "libhlld_b200.so")
 
 HLLD_OK = 0
-FP64, FP64_EXACT, MIXED = 0, 1, 2
-PRECISIONS = {"fp64": FP64, "fp64_exact": FP64_EXACT, "mixed": MIXED}
+FP64, FP64_EXACT, MIXED, FP32 = 0, 1, 2, 3
+PRECISIONS = {"fp64": FP64, "fp64_exact": FP64_EXACT, "mixed": MIXED, "fp32": FP32}
 SOLVERS = {"hlle": 0, "hlld": 1, "hllc": 2}
 EMF_MODES = {"solver": 0, "hll": 1}
 LIMITERS = {"pcm": 0, "mc": 1, "minmod": 2, "weno5z": 3, "mp5": 4, "mp7": 5}

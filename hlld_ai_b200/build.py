@@ -3,7 +3,8 @@
 ``python -m hlld_ai_b200.build`` (or ``build()``) compiles csrc/*.cu into
 object files under ``_build/`` and links the shared library next to this
 file, where ``hlld_ai_b200._lib`` loads it.  The FP64-exact variant is the
-same source as the FP64 one compiled with ``-fmad=false``.
+same source as the FP64 one compiled with ``-fmad=false``; the mixed and
+FP32 variants are the same source with float real types.
 """
 from __future__ import annotations
 
@@ -28,6 +29,7 @@ UNITS = [
     ("variant_fp64.cu", []),
     ("variant_exact.cu", ["-fmad=false"]),
     ("variant_mixed.cu", ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
+    ("variant_fp32.cu", ["-ftz=true"]),
     ("noalloc.cu", []),
     ("adjoint_fp64.cu", []),
 ]

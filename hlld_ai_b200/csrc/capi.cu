@@ -29,10 +29,15 @@ bool fp64_precision(int precision) {
     return precision == HLLD_FP64 || precision == HLLD_FP64_EXACT;
 }
 
-bool step_precision(int precision) { return fp64_precision(precision) || precision == HLLD_MIXED; }
+bool step_precision(int precision) {
+    return fp64_precision(precision) || precision == HLLD_MIXED || precision == HLLD_FP32;
+}
 
 // bytes of one element of the step's primitive, flux and EMF arrays
-size_t real_bytes(int precision) { return precision == HLLD_MIXED ? 4 : 8; }
+size_t real_bytes(int precision) { return (precision == HLLD_MIXED || precision == HLLD_FP32) ? 4 : 8; }
+// bytes of one element of the conserved state, the staggered field and the
+// RK stage-0 copy
+size_t state_bytes(int precision) { return precision == HLLD_FP32 ? 4 : 8; }
 
 int check_grid(const hlld_grid2d_t *g) {
     if (!g) return fail(HLLD_ERR_INVALID, "grid is NULL");
@@ -78,7 +83,7 @@ size_t layout_scratch(const hlld_grid2d_t *g, char *base, hlld::Scratch2D *sc) {
     const size_t nxt = g->nx + 2 * g->ng, nyt = g->ny + 2 * g->ng;
     const size_t nfx = (nxt + 1) * nyt, nfy = nxt * (nyt + 1), ncr = (nxt + 1) * (nyt + 1),
                  nc = nxt * nyt;
-    const size_t rb = real_bytes(g->precision);
+    const size_t rb = real_bytes(g->precision), sb = state_bytes(g->precision);
     size_t off = 0;
     auto take = [&](size_t count, size_t elem) -> void * {
         void *p = base ? (void *)(base + off) : nullptr;
@@ -89,9 +94,9 @@ size_t layout_scratch(const hlld_grid2d_t *g, char *base, hlld::Scratch2D *sc) {
     for (int k = 0; k < 7; ++k) s.Fx[k] = take(nfx, rb);
     for (int k = 0; k < 7; ++k) s.Fy[k] = take(nfy, rb);
     s.Ez = take(ncr, rb);
-    for (int k = 0; k < 6; ++k) s.U0[k] = (double *)take(nc, 8);
-    s.Bx0 = (double *)take(nfx, 8);
-    s.By0 = (double *)take(nfy, 8);
+    for (int k = 0; k < 6; ++k) s.U0[k] = (double *)take(nc, sb);
+    s.Bx0 = (double *)take(nfx, sb);
+    s.By0 = (double *)take(nfy, sb);
     s.diag = base ? (hlld_step_diag_t *)(base + off) : nullptr;
     off += align_up(sizeof(hlld_step_diag_t));
     // mixed form: the C2P roots of the step's first stage (warm start)
@@ -204,6 +209,8 @@ int hlld_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scrat
         hlld::v_exact::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
     else if (g->precision == HLLD_MIXED)
         hlld::v_mixed::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
+    else if (g->precision == HLLD_FP32)
+        hlld::v_fp32::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
     else
         hlld::v_fp64::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
     return check_launch("rk_step_ct");
@@ -221,6 +228,8 @@ int hlld_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *st
         hlld::v_exact::launch_sync_state(g, s, status, diag, st);
     else if (g->precision == HLLD_MIXED)
         hlld::v_mixed::launch_sync_state(g, s, status, diag, st);
+    else if (g->precision == HLLD_FP32)
+        hlld::v_fp32::launch_sync_state(g, s, status, diag, st);
     else
         hlld::v_fp64::launch_sync_state(g, s, status, diag, st);
     return check_launch("sync_state");
@@ -240,6 +249,8 @@ int hlld_sync_state_roots(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8
         hlld::v_exact::launch_sync_state(g, s, status, diag, st, mu_out, nullptr);
     else if (g->precision == HLLD_MIXED)
         hlld::v_mixed::launch_sync_state(g, s, status, diag, st, mu_out, mu_start);
+    else if (g->precision == HLLD_FP32)
+        hlld::v_fp32::launch_sync_state(g, s, status, diag, st, mu_out, mu_start);
     else
         hlld::v_fp64::launch_sync_state(g, s, status, diag, st, mu_out, nullptr);
     return check_launch("sync_state_roots");
@@ -275,6 +286,8 @@ int hlld_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, void
         hlld::v_exact::launch_sweep2d(g, s, axis, F, diag, st);
     else if (g->precision == HLLD_MIXED)
         hlld::v_mixed::launch_sweep2d(g, s, axis, F, diag, st);
+    else if (g->precision == HLLD_FP32)
+        hlld::v_fp32::launch_sweep2d(g, s, axis, F, diag, st);
     else
         hlld::v_fp64::launch_sweep2d(g, s, axis, F, diag, st);
     return check_launch("sweep2d");
@@ -309,6 +322,8 @@ int hlld_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *cons
         hlld::v_exact::launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
     else if (g->precision == HLLD_MIXED)
         hlld::v_mixed::launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
+    else if (g->precision == HLLD_FP32)
+        hlld::v_fp32::launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
     else
         hlld::v_fp64::launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
     return check_launch("ct_update2d");
@@ -354,6 +369,8 @@ int hlld_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
         hlld::v_exact::launch_tubes_run(b, cons, prims, U0, F, t_out, steps_out, next, threads, blocks, st);
     else if (b->precision == HLLD_MIXED)
         hlld::v_mixed::launch_tubes_run(b, cons, prims, U0, F, t_out, steps_out, next, threads, blocks, st);
+    else if (b->precision == HLLD_FP32)
+        hlld::v_fp32::launch_tubes_run(b, cons, prims, U0, F, t_out, steps_out, next, threads, blocks, st);
     else
         hlld::v_fp64::launch_tubes_run(b, cons, prims, U0, F, t_out, steps_out, next, threads, blocks, st);
     return check_launch("tubes_run");
@@ -371,6 +388,8 @@ int hlld_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double c
         hlld::v_exact::launch_compute_dt_2d(g, s, cfl, dt_dev, work, st);
     else if (g->precision == HLLD_MIXED)
         hlld::v_mixed::launch_compute_dt_2d(g, s, cfl, dt_dev, work, st);
+    else if (g->precision == HLLD_FP32)
+        hlld::v_fp32::launch_compute_dt_2d(g, s, cfl, dt_dev, work, st);
     else
         hlld::v_fp64::launch_compute_dt_2d(g, s, cfl, dt_dev, work, st);
     return check_launch("compute_dt_2d");

@@ -25,14 +25,19 @@
 #include "variants.h"
 
 // Real type of the 2D step's primitives, reconstruction, face fluxes, corner
-// EMF and flux divergence (double, or float for the mixed form), and of the
-// HLL-state C2P that seeds the HLLD p* bracket.  The p* iteration, the cell
-// C2P and the RK accumulation of the conserved state are always double.
+// EMF and flux divergence (double, or float for the mixed and FP32 forms), and
+// of the HLL-state C2P that seeds the HLLD p* bracket.
 #ifndef HLLD_REAL
 #define HLLD_REAL double
 #endif
 #ifndef HLLD_BRACKET_REAL
 #define HLLD_BRACKET_REAL HLLD_REAL
+#endif
+// Real type of the conserved state, the staggered field, the RK stage-0 copy,
+// the RK accumulation, the cell C2P and the HLLD p* iteration: double, or
+// float in the all-FP32 form.
+#ifndef HLLD_STATE_REAL
+#define HLLD_STATE_REAL double
 #endif
 
 namespace hlld {
@@ -40,12 +45,17 @@ namespace HLLD_NS {
 
 using R = HLLD_REAL;
 using RB = HLLD_BRACKET_REAL;
+using RS = HLLD_STATE_REAL;
 constexpr int kThreads = 128;
 // minimum resident blocks per SM requested for the sweep kernel (caps its
 // registers at 65536 / (kThreads * this))
 #ifndef HLLD_SWEEP_MIN_BLOCKS
 #define HLLD_SWEEP_MIN_BLOCKS 4
 #endif
+// The 2D sweeps and the tube kernel solve no p* on faces without normal
+// field (their HLLE fallback output does not depend on it), except in the
+// exact form, which keeps the reference's solver counters.
+constexpr bool kSkipBnZero = !HLLD_EXACT_ARITH;
 
 // ── small utilities ──────────────────────────────────────────────────────
 
@@ -335,7 +345,7 @@ enum { F_D = 0, F_SX, F_SY, F_SZ, F_TAU, F_BZ, F_BT, NFLUX };
 struct SweepParams {
     Grid g;
     const R *rho, *p, *vx, *vy, *vz, *bz;
-    const double *Bxf, *Byf;
+    const RS *Bxf, *Byf;
     R *F[NFLUX];
     hlld_flux_diag_t *diag;
     // optional per-face record for the adjoint: p* and the HLLE fallback
@@ -366,8 +376,8 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         // transverse in-plane B at cell c, averaged from its faces (ct.py:44-54)
         auto bt_at = [&](int c) -> T {
             return AXIS == 0
-                       ? T(0.5 * (p.Byf[(int64_t)c * (g.nyt + 1) + tr] + p.Byf[(int64_t)c * (g.nyt + 1) + tr + 1]))
-                       : T(0.5 * (p.Bxf[(int64_t)tr * g.nyt + c] + p.Bxf[(int64_t)(tr + 1) * g.nyt + c]));
+                       ? T(RS(0.5) * (p.Byf[(int64_t)c * (g.nyt + 1) + tr] + p.Byf[(int64_t)c * (g.nyt + 1) + tr + 1]))
+                       : T(RS(0.5) * (p.Bxf[(int64_t)tr * g.nyt + c] + p.Bxf[(int64_t)(tr + 1) * g.nyt + c]));
         };
         // work variables (reconstruction.py:269): rho, p, W vx, W vy, W vz,
         // transverse in-plane B, Bz
@@ -462,7 +472,7 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         }
         FaceOut<T> o;
         if (SOLVER == HLLD_SOLVER_HLLD)
-            hlld_face<AXIS, T, RB, double>(PL, PR, (T)g.gamma, false, o);
+            hlld_face<AXIS, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)g.gamma, false, o);
         else if (SOLVER == HLLD_SOLVER_HLLC)
             hllc_face<AXIS, T>(PL, PR, (T)g.gamma, false, o);
         else
@@ -511,7 +521,7 @@ template <typename T> __device__ __forceinline__ T upwind_sign(T F, T scale) {
 struct CtParams {
     Grid g;
     const R *vx, *vy;
-    const double *Bxf, *Byf;
+    const RS *Bxf, *Byf;
     const R *FxD, *FyD, *FxBt, *FyBt;
     const hlld_step_diag_t *diag;
     int upwind;
@@ -521,8 +531,8 @@ struct CtParams {
 // cell-centred E^z = v^y B^x - v^x B^y from face-averaged B (ct.py:44-60)
 __device__ __forceinline__ R cell_emf(const CtParams &p, int i, int j) {
     const int nyt = p.g.nyt;
-    R Bcx = R(0.5 * (p.Bxf[(int64_t)i * nyt + j] + p.Bxf[(int64_t)(i + 1) * nyt + j]));
-    R Bcy = R(0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]));
+    R Bcx = R(RS(0.5) * (p.Bxf[(int64_t)i * nyt + j] + p.Bxf[(int64_t)(i + 1) * nyt + j]));
+    R Bcy = R(RS(0.5) * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]));
     int64_t c = (int64_t)i * nyt + j;
     return Bcx * p.vy[c] - Bcy * p.vx[c];
 }
@@ -568,9 +578,9 @@ __global__ void __launch_bounds__(kThreads) ct_emf_kernel(const CtParams p) {
 
 struct UpdateParams {
     Grid g;
-    double *U[6];
-    double *U0[6];
-    double *Bxf, *Byf, *Bx0, *By0;
+    RS *U[6];
+    RS *U0[6];
+    RS *Bxf, *Byf, *Bx0, *By0;
     const R *Fx[6];
     const R *Fy[6];
     const R *Ez;
@@ -580,7 +590,7 @@ struct UpdateParams {
     int first_stage;
 };
 
-// flux divergence (in R) + CT face update + RK combine (in double) on the
+// flux divergence (in R) + CT face update + RK combine (in RS) on the
 // physical block and its upper faces; a thread owns cell (i, j), face
 // Bxf(i, j) and face Byf(i, j)
 __global__ void __launch_bounds__(kThreads) ct_update_kernel(const UpdateParams p) {
@@ -591,7 +601,8 @@ __global__ void __launch_bounds__(kThreads) ct_update_kernel(const UpdateParams 
     const int ii = (int)(e / (g.ny + 1)), jj = (int)(e - (int64_t)ii * (g.ny + 1));
     const int i = g.ng + ii, j = g.ng + jj;
     const double dt = p.dt_dev ? *p.dt_dev : p.dt_host;
-    const double w2 = p.c * dt;
+    const RS w2 = RS(p.c * dt);
+    const RS a = RS(p.a), b = RS(p.b);
     const R rdx = R(g.dx), rdy = R(g.dy);
     if (ii < g.nx && jj < g.ny) {
         const int64_t c = (int64_t)i * nyt + j;
@@ -599,50 +610,50 @@ __global__ void __launch_bounds__(kThreads) ct_update_kernel(const UpdateParams 
         for (int k = 0; k < 6; ++k) {
             R rx = -(p.Fx[k][(int64_t)(i + 1) * nyt + j] - p.Fx[k][c]) / rdx;
             R ry = -(p.Fy[k][(int64_t)i * (nyt + 1) + j + 1] - p.Fy[k][(int64_t)i * (nyt + 1) + j]) / rdy;
-            double L = (double)(rx + ry);
-            double u = p.U[k][c];
-            double u0;
+            RS L = (RS)(rx + ry);
+            RS u = p.U[k][c];
+            RS u0;
             if (p.first_stage) {
                 u0 = u;
                 p.U0[k][c] = u;
             } else {
                 u0 = p.U0[k][c];
             }
-            double v = p.a * u0;
-            v = v + p.b * u;
+            RS v = a * u0;
+            v = v + b * u;
             v = v + w2 * L;
             p.U[k][c] = v;
         }
     }
     if (jj < g.ny) {
         const int64_t fx = (int64_t)i * nyt + j;
-        double dB = ((double)p.Ez[(int64_t)i * (nyt + 1) + j] - (double)p.Ez[(int64_t)i * (nyt + 1) + j + 1]) / g.dy;
-        double u = p.Bxf[fx];
-        double u0;
+        RS dB = ((RS)p.Ez[(int64_t)i * (nyt + 1) + j] - (RS)p.Ez[(int64_t)i * (nyt + 1) + j + 1]) / RS(g.dy);
+        RS u = p.Bxf[fx];
+        RS u0;
         if (p.first_stage) {
             u0 = u;
             p.Bx0[fx] = u;
         } else {
             u0 = p.Bx0[fx];
         }
-        double v = p.a * u0;
-        v = v + p.b * u;
+        RS v = a * u0;
+        v = v + b * u;
         v = v + w2 * dB;
         p.Bxf[fx] = v;
     }
     if (ii < g.nx) {
         const int64_t fy = (int64_t)i * (nyt + 1) + j;
-        double dB = ((double)p.Ez[(int64_t)(i + 1) * (nyt + 1) + j] - (double)p.Ez[(int64_t)i * (nyt + 1) + j]) / g.dx;
-        double u = p.Byf[fy];
-        double u0;
+        RS dB = ((RS)p.Ez[(int64_t)(i + 1) * (nyt + 1) + j] - (RS)p.Ez[(int64_t)i * (nyt + 1) + j]) / RS(g.dx);
+        RS u = p.Byf[fy];
+        RS u0;
         if (p.first_stage) {
             u0 = u;
             p.By0[fy] = u;
         } else {
             u0 = p.By0[fy];
         }
-        double v = p.a * u0;
-        v = v + p.b * u;
+        RS v = a * u0;
+        v = v + b * u;
         v = v + w2 * dB;
         p.Byf[fy] = v;
     }
@@ -708,8 +719,8 @@ __global__ void __launch_bounds__(kThreads) ghost_kernel(const GhostParams<E> p)
 
 struct C2PCellsParams {
     Grid g;
-    const double *U[6];
-    const double *Bxf, *Byf;
+    const RS *U[6];
+    const RS *Bxf, *Byf;
     R *P[9];
     uint8_t *status;
     hlld_step_diag_t *diag;
@@ -719,16 +730,17 @@ struct C2PCellsParams {
 
 // Kastaun's root mu = 1 / (h W) of a cell's primitives (h = 1 + eps + p / rho),
 // or 0 -- no start, the bracketed solve -- where they are not physical
-__device__ __forceinline__ double kastaun_mu_of_prims(const R *const *P, int64_t c) {
-    const double rho = P[P_RHO][c], press = P[P_P][c], eps = P[P_EPS][c];
-    const double vx = P[P_VX][c], vy = P[P_VY][c], vz = P[P_VZ][c];
-    const double v2 = vx * vx + vy * vy + vz * vz;
-    const double h = 1.0 + eps + press / rho;
-    return (v2 < 1.0 && rho > 0.0 && h > 0.0) ? sqrt(1.0 - v2) / h : 0.0;
+template <typename T>
+__device__ __forceinline__ T kastaun_mu_of_prims(const R *const *P, int64_t c) {
+    const T rho = P[P_RHO][c], press = P[P_P][c], eps = P[P_EPS][c];
+    const T vx = P[P_VX][c], vy = P[P_VY][c], vz = P[P_VZ][c];
+    const T v2 = vx * vx + vy * vy + vz * vz;
+    const T h = T(1) + eps + press / rho;
+    return (v2 < T(1) && rho > T(0) && h > T(0)) ? sqrt(T(1) - v2) / h : T(0);
 }
 
 // cell-centred B (ct.py:44-54) + C2P (c2p.py:313-363) of the physical cells,
-// in double; primitives stored as R.  FROM_PRIMS: each root search starts
+// in RS; primitives stored as R.  FROM_PRIMS: each root search starts
 // from the root of the cell's current primitives, which the kernel then
 // overwrites (a template flag: a runtime one made the other launches 5 %
 // slower)
@@ -741,18 +753,18 @@ __global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParam
         const int i = g.ng + (int)(e / g.ny), j = g.ng + (int)(e % g.ny);
         const int nyt = g.nyt;
         const int64_t c = (int64_t)i * nyt + j;
-        double Bcx = 0.5 * (p.Bxf[c] + p.Bxf[(int64_t)(i + 1) * nyt + j]);
-        double Bcy = 0.5 * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
-        double C[NCONS] = {p.U[0][c], p.U[1][c], p.U[2][c], p.U[3][c], p.U[4][c], Bcx, Bcy, p.U[5][c]};
-        double P[NPRIM];
-        double mu = 0.0;
-        double mu0 = 0.0;
-        if constexpr (FROM_PRIMS) mu0 = kastaun_mu_of_prims(p.P, c);
-        else if (p.mu_warm) mu0 = p.mu_warm[c];
-        uint8_t st = cons_to_prim<double>(C, g.gamma, g.atmo_rho, 1e-10, P,
-                                          (p.mu_out || p.mu_warm) ? &mu : nullptr, mu0);
-        if (p.mu_out) p.mu_out[c] = mu;
-        if (p.mu_warm) p.mu_warm[c] = mu;
+        RS Bcx = RS(0.5) * (p.Bxf[c] + p.Bxf[(int64_t)(i + 1) * nyt + j]);
+        RS Bcy = RS(0.5) * (p.Byf[(int64_t)i * (nyt + 1) + j] + p.Byf[(int64_t)i * (nyt + 1) + j + 1]);
+        RS C[NCONS] = {p.U[0][c], p.U[1][c], p.U[2][c], p.U[3][c], p.U[4][c], Bcx, Bcy, p.U[5][c]};
+        RS P[NPRIM];
+        RS mu = RS(0);
+        RS mu0 = RS(0);
+        if constexpr (FROM_PRIMS) mu0 = kastaun_mu_of_prims<RS>(p.P, c);
+        else if (p.mu_warm) mu0 = (RS)p.mu_warm[c];
+        uint8_t st = cons_to_prim<RS>(C, RS(g.gamma), RS(g.atmo_rho), RS(1e-10), P,
+                                      (p.mu_out || p.mu_warm) ? &mu : nullptr, mu0);
+        if (p.mu_out) p.mu_out[c] = (double)mu;
+        if (p.mu_warm) p.mu_warm[c] = (double)mu;
 #pragma unroll
         for (int k = 0; k < NPRIM; ++k) p.P[k][c] = (R)P[k];
         if (p.status) p.status[c] = st;
@@ -838,18 +850,23 @@ struct TubesParams {
     const double *dx;
     const int32_t *order;
     double cfl, tend, gamma, atmo_rho;
-    double *U[8];   // conserved, all eight components
-    double *U0[8];
+    RS *U[8];   // conserved, all eight components
+    RS *U0[8];
     R *P[9];        // primitives
     R *F[8];        // face fluxes (slot C_BX unused: F[Bx] = 0)
     double *t_out;
     int32_t *steps_out;
     unsigned int *next;
+    int smem_faces;  // faces whose seven fluxes fit the CTA's dynamic shared memory
 };
+
+// The seven flux slots of a tube face (F[Bx] = 0 is never stored): slot of
+// conserved component k
+__device__ __forceinline__ int tube_flux_slot(int k) { return k < C_BX ? k : k - 1; }
 
 template <int LIM, int SOLVER>
 __device__ __forceinline__ void tube_face(const TubesParams &p, int64_t base, int nt, int f,
-                                          int64_t fout) {
+                                          R *const *Ft) {
     using T = R;
     constexpr int S = Stencil<LIM>::S;
     constexpr int NW = 2 * S + 2;
@@ -929,12 +946,12 @@ __device__ __forceinline__ void tube_face(const TubesParams &p, int64_t base, in
     }
     FaceOut<T> o;
     if (SOLVER == HLLD_SOLVER_HLLD)
-        hlld_face<0, T, RB, double>(PL, PR, (T)p.gamma, false, o);
+        hlld_face<0, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)p.gamma, false, o);
     else
         hlle_face<0, T>(PL, PR, (T)p.gamma, false, false, o);
 #pragma unroll
     for (int k = 0; k < 8; ++k)
-        if (k != C_BX) p.F[k][fout] = o.F[k];
+        if (k != C_BX) Ft[tube_flux_slot(k)][f] = o.F[k];
 }
 
 // One physical face of the 1D shock-tube driver (driver.py:130-189,
@@ -942,7 +959,7 @@ __device__ __forceinline__ void tube_face(const TubesParams &p, int64_t base, in
 // as it is along the whole line (no W v, no positivity fallback, no floors).
 template <int LIM, int SOLVER>
 __device__ __forceinline__ void tube_face_driver1d(const TubesParams &p, int64_t base, int nt, int f,
-                                                   int64_t fout) {
+                                                   R *const *Ft) {
     using T = R;
     constexpr int S = Stencil<LIM>::S;
     constexpr int NW = 2 * S + 2;
@@ -963,12 +980,12 @@ __device__ __forceinline__ void tube_face_driver1d(const TubesParams &p, int64_t
     }
     FaceOut<T> o;
     if (SOLVER == HLLD_SOLVER_HLLD)
-        hlld_face<0, T, RB, double>(PL, PR, (T)p.gamma, false, o);
+        hlld_face<0, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)p.gamma, false, o);
     else
         hlle_face<0, T>(PL, PR, (T)p.gamma, false, false, o);
 #pragma unroll
     for (int k = 0; k < 8; ++k)
-        if (k != C_BX) p.F[k][fout] = o.F[k];
+        if (k != C_BX) Ft[tube_flux_slot(k)][f] = o.F[k];
 }
 
 __device__ __forceinline__ unsigned long long block_max_any(unsigned long long x,
@@ -999,9 +1016,17 @@ template <int LIM, int SOLVER, bool DRV>
 // keeps all its warps in the same phase of the tube (faces, update, C2P),
 // which the instruction cache rewards (measured on B200: +26 % over two CTAs
 // of 256 on the batched workload).
+//
+// A stage is two passes separated by block barriers: the faces (fluxes into
+// shared memory when the tube's faces fit, else into the face arrays), then
+// per physical cell the RK update, the C2P and the outflow copies into the
+// ghost cells that this cell feeds.  The fused second pass reads and writes
+// each cell's state once per stage; its arithmetic is that of the separate
+// update, boundary, C2P and boundary passes of the reference's stage.
 __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
     __shared__ unsigned long long red[33];
     __shared__ int s_tube;
+    extern __shared__ __align__(16) unsigned char tube_smem[];
     const int ng = p.ng;
     for (;;) {
         if (threadIdx.x == 0) s_tube = (int)atomicAdd(p.next, 1u);
@@ -1015,12 +1040,23 @@ __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
         const int64_t base = p.cell_off[ti];
         const int64_t fbase = base + ti;  // tube ti has nt + 1 faces
         const double dx = p.dx[ti];
+        R *Ft[7];  // the tube's flux slots, indexed by face 0 .. nt
+        {
+            const bool in_smem = nt + 1 <= p.smem_faces;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                if (k == C_BX) continue;
+                const int sl = tube_flux_slot(k);
+                Ft[sl] = in_smem ? reinterpret_cast<R *>(tube_smem) + (int64_t)sl * (nt + 1)
+                                 : p.F[k] + fbase;
+            }
+        }
         // conserved variables from the primitives (hlld.py:185-217)
         for (int c = threadIdx.x; c < nt && !p.resume; c += blockDim.x) {
-            double Pd[NPRIM], Cd[NCONS];
+            RS Pd[NPRIM], Cd[NCONS];
 #pragma unroll
-            for (int k = 0; k < NPRIM; ++k) Pd[k] = (double)p.P[k][base + c];
-            prim_to_cons<double>(Pd, Cd);
+            for (int k = 0; k < NPRIM; ++k) Pd[k] = (RS)p.P[k][base + c];
+            prim_to_cons<RS>(Pd, Cd);
 #pragma unroll
             for (int k = 0; k < NCONS; ++k) p.U[k][base + c] = Cd[k];
         }
@@ -1058,7 +1094,7 @@ __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
             // arrays may alias for all the compiler knows, so a load after a
             // store would wait for it, one memory latency per variable)
             for (int c = threadIdx.x; c < nt; c += blockDim.x) {
-                double u[8];
+                RS u[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) u[k] = p.U[k][base + c];
 #pragma unroll
@@ -1066,87 +1102,79 @@ __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
             }
             for (int st = 0; st < nst; ++st) {
                 const double *w = p.scheme == 3 ? kRK3d[st] : kRK2d[st];
-                const double w2 = w[2] * dt;
+                const RS w0 = RS(w[0]), w1 = RS(w[1]), w2 = RS(w[2] * dt);
+                const RS rdt = RS(dt);
                 if (DRV) {
                     // physical faces ng .. ng + L (reconstruction.py:354-373)
                     for (int f = ng + threadIdx.x; f <= ng + L; f += blockDim.x)
-                        tube_face_driver1d<LIM, SOLVER>(p, base, nt, f, fbase + f);
+                        tube_face_driver1d<LIM, SOLVER>(p, base, nt, f, Ft);
                 } else {
                     for (int f = threadIdx.x; f <= nt; f += blockDim.x)
-                        tube_face<LIM, SOLVER>(p, base, nt, f, fbase + f);
+                        tube_face<LIM, SOLVER>(p, base, nt, f, Ft);
                 }
                 __syncthreads();
-                // Heun (driver.py:223-232): U1 = U + dt L(U); U' = 0.5 (U + U1 + dt L(U1)),
-                // with rhs = (F_c - F_c+1) / dx on the physical cells; Bx held
-                for (int c = ng + threadIdx.x; DRV && c < ng + L; c += blockDim.x) {
+                // per physical cell: the update -- Heun (driver.py:223-232): U1 = U
+                // + dt L(U), U' = 0.5 (U + U1 + dt L(U1)), rhs = (F_c - F_c+1) / dx,
+                // Bx held; or the SSP-RK combine of rk_step with F[Bx] = 0 --
+                // then the C2P, then the outflow copies (grid.py:93-113) of U
+                // and of the primitives into the ghost cells next to an edge
+                for (int c = ng + threadIdx.x; c < ng + L; c += blockDim.x) {
                     const int64_t ci = base + c;
-                    double rhs[8], u0[8], u[8];
+                    RS u0[8], u[8];
+                    R fl[8], fr[8];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        if (k == C_BX) continue;
-                        rhs[k] = (double)((p.F[k][fbase + c] - p.F[k][fbase + c + 1]) / R(dx));
                         u0[k] = p.U0[k][ci];
                         u[k] = p.U[k][ci];
-                    }
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        if (k == C_BX) continue;
-                        p.U[k][ci] = st == 0 ? u0[k] + dt * rhs[k] : 0.5 * (u0[k] + u[k] + dt * rhs[k]);
-                    }
-                }
-                for (int c = threadIdx.x; !DRV && c < nt; c += blockDim.x) {
-                    double rhs[8], u0[8], u[8];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        if (k == C_BX) {
-                            rhs[k] = -(0.0 - 0.0) / dx + (-0.0);
-                        } else {
-                            R d = p.F[k][fbase + c + 1] - p.F[k][fbase + c];
-                            rhs[k] = (double)(-d / R(dx)) + (-0.0);
+                        if (k != C_BX) {
+                            fl[k] = Ft[tube_flux_slot(k)][c];
+                            fr[k] = Ft[tube_flux_slot(k)][c + 1];
                         }
-                        u0[k] = p.U0[k][base + c];
-                        u[k] = p.U[k][base + c];
                     }
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        double v = w[0] * u0[k] + w[1] * u[k];
-                        p.U[k][base + c] = v + w2 * rhs[k];
-                    }
-                }
-                __syncthreads();
-                // outflow BCs on the conserved variables (grid.py:93-113)
-                for (int c = threadIdx.x; c < 2 * ng; c += blockDim.x) {
-                    const int gc = c < ng ? c : L + c;
-                    const int sc = c < ng ? ng : ng + L - 1;
-                    double u[8];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) u[k] = p.U[k][base + sc];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) p.U[k][base + gc] = u[k];
-                }
-                __syncthreads();
-                for (int c = ng + threadIdx.x; c < ng + L; c += blockDim.x) {
-                    double Cd[NCONS], Pd[NPRIM];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) Cd[k] = p.U[k][base + c];
                     // mixed form: the root search starts from the root of the
                     // cell's primitives before the stage, which this C2P
                     // overwrites (the 2D step's first-stage start)
-                    double mu0 = 0.0;
-                    if constexpr (sizeof(R) == sizeof(float)) mu0 = kastaun_mu_of_prims(p.P, base + c);
-                    cons_to_prim<double>(Cd, p.gamma, p.atmo_rho, 1e-10, Pd, nullptr, mu0);
+                    RS mu0 = RS(0);
+                    if constexpr (sizeof(R) == sizeof(float) && sizeof(RS) == sizeof(double))
+                        mu0 = kastaun_mu_of_prims<RS>(p.P, ci);
+                    RS un[8];
 #pragma unroll
-                    for (int k = 0; k < NPRIM; ++k) p.P[k][base + c] = (R)Pd[k];
-                }
-                __syncthreads();
-                for (int c = threadIdx.x; c < 2 * ng; c += blockDim.x) {
-                    const int gc = c < ng ? c : L + c;
-                    const int sc = c < ng ? ng : ng + L - 1;
-                    R q[NPRIM];
+                    for (int k = 0; k < 8; ++k) {
+                        if (DRV) {
+                            if (k == C_BX) {
+                                un[k] = u[k];
+                                continue;
+                            }
+                            const RS rhs = (RS)((fl[k] - fr[k]) / R(dx));
+                            un[k] = st == 0 ? u0[k] + rdt * rhs : RS(0.5) * (u0[k] + u[k] + rdt * rhs);
+                        } else {
+                            RS rhs;
+                            if (k == C_BX) {
+                                rhs = -(RS(0) - RS(0)) / RS(dx) + RS(-0.0);
+                            } else {
+                                const R d = fr[k] - fl[k];
+                                rhs = (RS)(-d / R(dx)) + RS(-0.0);
+                            }
+                            const RS v = w0 * u0[k] + w1 * u[k];
+                            un[k] = v + w2 * rhs;
+                        }
+                    }
+                    RS Pd[NPRIM];
+                    cons_to_prim<RS>(un, RS(p.gamma), RS(p.atmo_rho), RS(1e-10), Pd, nullptr, mu0);
 #pragma unroll
-                    for (int k = 0; k < NPRIM; ++k) q[k] = p.P[k][base + sc];
+                    for (int k = 0; k < 8; ++k) p.U[k][ci] = un[k];
 #pragma unroll
-                    for (int k = 0; k < NPRIM; ++k) p.P[k][base + gc] = q[k];
+                    for (int k = 0; k < NPRIM; ++k) p.P[k][ci] = (R)Pd[k];
+                    for (int side = 0; side < 2; ++side) {
+                        if (c != (side == 0 ? ng : ng + L - 1)) continue;
+                        const int g0 = side == 0 ? 0 : ng + L;
+                        for (int gc = g0; gc < g0 + ng; ++gc) {
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) p.U[k][base + gc] = un[k];
+#pragma unroll
+                            for (int k = 0; k < NPRIM; ++k) p.P[k][base + gc] = (R)Pd[k];
+                        }
+                    }
                 }
                 __syncthreads();
             }
@@ -1292,9 +1320,9 @@ static void launch_ghost_cc(const Grid &G, E *const *arrs, int narr, cudaStream_
     ghost_kernel<E><<<dim3(grid1d(cnt), narr), kThreads, 0, st>>>(gp);
 }
 
-static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStream_t st) {
+static void launch_ghost_faces(const Grid &G, RS *Bxf, RS *Byf, cudaStream_t st) {
     // Bxf: face rule along x, cell rule along y (grid.py:250-251)
-    GhostParams<double> gp = {};
+    GhostParams<RS> gp = {};
     gp.v[0] = Bxf;
     gp.n0 = G.nxt + 1;
     gp.n1 = G.nyt;
@@ -1310,9 +1338,9 @@ static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStre
     gp.face0 = 1;
     gp.face1 = 0;
     int64_t cnt = (int64_t)gp.n0 * gp.n1 - (int64_t)(gp.b0 - gp.a0) * (gp.b1 - gp.a1);
-    ghost_kernel<double><<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gp);
+    ghost_kernel<RS><<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gp);
     // Byf: cell rule along x, face rule along y (grid.py:253-254)
-    GhostParams<double> gq = {};
+    GhostParams<RS> gq = {};
     gq.v[0] = Byf;
     gq.n0 = G.nxt;
     gq.n1 = G.nyt + 1;
@@ -1328,24 +1356,24 @@ static void launch_ghost_faces(const Grid &G, double *Bxf, double *Byf, cudaStre
     gq.face0 = 0;
     gq.face1 = 1;
     cnt = (int64_t)gq.n0 * gq.n1 - (int64_t)(gq.b0 - gq.a0) * (gq.b1 - gq.a1);
-    ghost_kernel<double><<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gq);
+    ghost_kernel<RS><<<dim3(grid1d(cnt), 1), kThreads, 0, st>>>(gq);
 }
 
 void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
                        hlld_step_diag_t *diag, cudaStream_t st, double *mu_out, double *mu_warm,
                        bool start_from_prims) {
     Grid G = make_grid(g);
-    double *cons[6];
-    for (int k = 0; k < 6; ++k) cons[k] = (double *)s->cons[k];
+    RS *cons[6];
+    for (int k = 0; k < 6; ++k) cons[k] = (RS *)s->cons[k];
     R *prims[9];
     for (int k = 0; k < 9; ++k) prims[k] = (R *)s->prims[k];
-    launch_ghost_faces(G, (double *)s->Bxf, (double *)s->Byf, st);
-    launch_ghost_cc<double>(G, cons, 6, st);
+    launch_ghost_faces(G, (RS *)s->Bxf, (RS *)s->Byf, st);
+    launch_ghost_cc<RS>(G, cons, 6, st);
     C2PCellsParams cp = {};
     cp.g = G;
     for (int k = 0; k < 6; ++k) cp.U[k] = cons[k];
-    cp.Bxf = (const double *)s->Bxf;
-    cp.Byf = (const double *)s->Byf;
+    cp.Bxf = (const RS *)s->Bxf;
+    cp.Byf = (const RS *)s->Byf;
     for (int k = 0; k < 9; ++k) cp.P[k] = prims[k];
     cp.status = status;
     cp.diag = diag;
@@ -1370,8 +1398,8 @@ void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis, v
     sp.vy = (const R *)s->prims[P_VY];
     sp.vz = (const R *)s->prims[P_VZ];
     sp.bz = (const R *)s->prims[P_BZ];
-    sp.Bxf = (const double *)s->Bxf;
-    sp.Byf = (const double *)s->Byf;
+    sp.Bxf = (const RS *)s->Bxf;
+    sp.Byf = (const RS *)s->Byf;
     for (int k = 0; k < NFLUX; ++k) sp.F[k] = (R *)F[k];
     sp.diag = fdiag;
     if (axis == 0) launch_sweep<0>(g->limiter, g->solver, sp, st);
@@ -1392,8 +1420,8 @@ void launch_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, const S
     cp.g = G;
     cp.vx = (const R *)s->prims[P_VX];
     cp.vy = (const R *)s->prims[P_VY];
-    cp.Bxf = (const double *)s->Bxf;
-    cp.Byf = (const double *)s->Byf;
+    cp.Bxf = (const RS *)s->Bxf;
+    cp.Byf = (const RS *)s->Byf;
     cp.FxD = (const R *)sc.Fx[F_D];
     cp.FyD = (const R *)sc.Fy[F_D];
     cp.FxBt = (const R *)sc.Fx[F_BT];
@@ -1405,15 +1433,15 @@ void launch_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, const S
     UpdateParams up = {};
     up.g = G;
     for (int k = 0; k < 6; ++k) {
-        up.U[k] = (double *)s->cons[k];
-        up.U0[k] = sc.U0[k];
+        up.U[k] = (RS *)s->cons[k];
+        up.U0[k] = (RS *)sc.U0[k];
         up.Fx[k] = (const R *)sc.Fx[k];
         up.Fy[k] = (const R *)sc.Fy[k];
     }
-    up.Bxf = (double *)s->Bxf;
-    up.Byf = (double *)s->Byf;
-    up.Bx0 = sc.Bx0;
-    up.By0 = sc.By0;
+    up.Bxf = (RS *)s->Bxf;
+    up.Byf = (RS *)s->Byf;
+    up.Bx0 = (RS *)sc.Bx0;
+    up.By0 = (RS *)sc.By0;
     up.Ez = (const R *)sc.Ez;
     up.dt_dev = dt_dev;
     up.dt_host = dt_host;
@@ -1445,15 +1473,41 @@ void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Sc
     }
 }
 
+// Dynamic shared memory of a tube CTA for the fluxes of its tube: at most
+// 120 KB (the faces of a 4096-cell tube in the FP32 flux types), and no more
+// than the SM's share for the CTAs that run on it, so that the stencil loads
+// keep the rest of the SM's 256 KB of L1 / shared memory as cache.
+static constexpr int kTubeSmemCap = 120 * 1024;
+
+template <typename K>
+static void tube_launch(K kernel, TubesParams tp, int blocks, int threads, cudaStream_t st) {
+    int dev = 0, sms = 1, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    const int ctas_per_sm = (blocks + sms - 1) / (sms > 0 ? sms : 1);
+    int bytes = per_sm / (ctas_per_sm > 0 ? ctas_per_sm : 1) - 2048;  // static shared and reserve
+    if (bytes > kTubeSmemCap) bytes = kTubeSmemCap;
+    if (bytes < 0) bytes = 0;
+    tp.smem_faces = bytes / (7 * (int)sizeof(R));
+    bytes = tp.smem_faces * 7 * (int)sizeof(R);
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+        cudaGetLastError();  // clear it: fall back to the face arrays
+        tp.smem_faces = 0;
+        bytes = 0;
+    }
+    kernel<<<blocks, threads, bytes, st>>>(tp);
+}
+
 template <int LIM>
 static void launch_tubes_lim(int solver, bool drv, const TubesParams &tp, int blocks, int threads,
                              cudaStream_t st) {
     if (solver == HLLD_SOLVER_HLLD) {
-        if (drv) tubes_kernel<LIM, HLLD_SOLVER_HLLD, true><<<blocks, threads, 0, st>>>(tp);
-        else tubes_kernel<LIM, HLLD_SOLVER_HLLD, false><<<blocks, threads, 0, st>>>(tp);
+        if (drv) tube_launch(tubes_kernel<LIM, HLLD_SOLVER_HLLD, true>, tp, blocks, threads, st);
+        else tube_launch(tubes_kernel<LIM, HLLD_SOLVER_HLLD, false>, tp, blocks, threads, st);
     } else {
-        if (drv) tubes_kernel<LIM, HLLD_SOLVER_HLLE, true><<<blocks, threads, 0, st>>>(tp);
-        else tubes_kernel<LIM, HLLD_SOLVER_HLLE, false><<<blocks, threads, 0, st>>>(tp);
+        if (drv) tube_launch(tubes_kernel<LIM, HLLD_SOLVER_HLLE, true>, tp, blocks, threads, st);
+        else tube_launch(tubes_kernel<LIM, HLLD_SOLVER_HLLE, false>, tp, blocks, threads, st);
     }
 }
 
@@ -1477,8 +1531,8 @@ void launch_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *pri
     tp.gamma = b->gamma;
     tp.atmo_rho = b->atmo_rho;
     for (int k = 0; k < 8; ++k) {
-        tp.U[k] = (double *)cons[k];
-        tp.U0[k] = (double *)U0[k];
+        tp.U[k] = (RS *)cons[k];
+        tp.U0[k] = (RS *)U0[k];
         tp.F[k] = (R *)F[k];
     }
     for (int k = 0; k < 9; ++k) tp.P[k] = (R *)prims[k];

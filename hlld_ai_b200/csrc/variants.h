@@ -2,7 +2,7 @@
 // v_fp64: FP64 with FMA contraction; v_exact: FP64 with one rounding per
 // operation (translation unit built with -fmad=false); v_mixed: FP32
 // primitives, reconstruction, fluxes, EMF and divergence, FP64 cell C2P,
-// HLLD p* iteration and RK accumulation.
+// HLLD p* iteration and RK accumulation; v_fp32: FP32 throughout.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,7 +16,7 @@ struct Scratch2D {
     void *Fx[7];  // x-face fluxes: D, Sx, Sy, Sz, tau, Bz, By (the variant's real type)
     void *Fy[7];  // y-face fluxes: D, Sx, Sy, Sz, tau, Bz, Bx
     void *Ez;     // corner EMF (the variant's real type)
-    double *U0[6];  // RK stage-0 copy of the evolved cell variables
+    double *U0[6];  // RK stage-0 copy of the evolved cell variables (float in the FP32 form)
     double *Bx0, *By0;
     hlld_step_diag_t *diag;  // used when the caller passes none
     double *mu_warm;         // mixed form: each cell's last C2P root (warm start), or NULL
@@ -73,5 +73,6 @@ void launch_prim_to_cons_vjp(int64_t n, const void *const *prim, const void *con
 }
 HLLD_DECLARE_VARIANT(v_exact)
 HLLD_DECLARE_VARIANT(v_mixed)
+HLLD_DECLARE_VARIANT(v_fp32)
 
 }  // namespace hlld

@@ -88,7 +88,7 @@ class TubeBatch:
                  ng: int | None = None):
         from .physics.reconstruction import ghosts_needed
 
-        if precision not in ("fp64", "fp64_exact", "mixed"):
+        if precision not in ("fp64", "fp64_exact", "mixed", "fp32"):
             raise ValueError(f"unknown precision {precision!r}")
         if flavor not in FLAVORS:
             raise ValueError(f"unknown flavor {flavor!r}")
@@ -114,11 +114,13 @@ class TubeBatch:
             for k in PRIM_KEYS:
                 host[k][off[i]:off[i + 1]] = p[k]
         self.host_init = host
-        self.pdtype = torch.float32 if precision == "mixed" else torch.float64
+        self.pdtype = torch.float32 if precision in ("mixed", "fp32") else torch.float64
+        # conserved state: float32 in the all-FP32 form only
+        self.sdtype = torch.float32 if precision == "fp32" else torch.float64
         dev = self.device
         self.prims = {k: torch.tensor(host[k], dtype=self.pdtype, device=dev) for k in PRIM_KEYS}
-        self.cons = [torch.empty(self.total_cells, dtype=torch.float64, device=dev) for _ in range(8)]
-        self.U0 = [torch.empty(self.total_cells, dtype=torch.float64, device=dev) for _ in range(8)]
+        self.cons = [torch.empty(self.total_cells, dtype=self.sdtype, device=dev) for _ in range(8)]
+        self.U0 = [torch.empty(self.total_cells, dtype=self.sdtype, device=dev) for _ in range(8)]
         self.F = [torch.empty(self.total_faces, dtype=self.pdtype, device=dev) for _ in range(8)]
         self.ncells = torch.tensor(L.astype(np.int32), device=dev)
         self.cell_off = torch.tensor(off[:-1], device=dev)

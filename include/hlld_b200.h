@@ -7,8 +7,9 @@
  *   - All array arguments are DEVICE pointers to contiguous row-major
  *     arrays; no entry point allocates device memory except where stated.
  *   - Real arrays are double for HLLD_FP64 / HLLD_FP64_EXACT; for
- *     HLLD_MIXED the primitive arrays are float and everything else double
- *     (see each entry point).
+ *     HLLD_MIXED the primitive arrays are float and everything else double;
+ *     for HLLD_FP32 every state array (conserved, primitive, staggered
+ *     field) is float (see each entry point).
  *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Every
  *     entry point only enqueues work; nothing synchronises the host.
  *   - Return value: HLLD_OK or a negative HLLD_ERR_* code;
@@ -40,7 +41,9 @@ extern "C" {
 enum hlld_precision {
     HLLD_FP64 = 0,       /* FP64 throughout, FMA contraction on */
     HLLD_FP64_EXACT = 1, /* FP64, one rounding per operation (reference order) */
-    HLLD_MIXED = 2       /* FP32 reconstruction/fluxes/update, FP64 C2P, p*, RK state */
+    HLLD_MIXED = 2,      /* FP32 reconstruction/fluxes/update, FP64 C2P, p*, RK state */
+    HLLD_FP32 = 3        /* FP32 throughout: every array and every root solve in float
+                          * (2D step and tube kernel only) */
 };
 /* HLLE: hlld.py:1005-1044; HLLD: :1202-1543; HLLC: :1549-1765 (flux plugin
  * and 2D step; the tube kernel and the adjoint take HLLE and HLLD) */
@@ -63,9 +66,9 @@ enum hlld_bc { HLLD_BC_OUTFLOW = 0, HLLD_BC_PERIODIC = 1 };
 #define HLLD_RF_FAILED 4u
 
 /* Device-resident counters of one flux sweep: the numbers the reference
- * keeps in hlld.LAST_DIAG (src/physics/hlld.py:1516-1529).  In HLLD_MIXED
- * the sweep does not solve p* on faces with B_n = 0, whose HLLE fallback
- * result does not depend on it.  Those faces count in n_faces, n_bn_zero
+ * keeps in hlld.LAST_DIAG (src/physics/hlld.py:1516-1529).  In every form
+ * but HLLD_FP64_EXACT the 2D sweep does not solve p* on faces with B_n = 0,
+ * whose HLLE fallback result does not depend on it.  Those faces count in n_faces, n_bn_zero
  * and n_failed only, so n_not_converged, n_wave_order_bad, iters_sum_conv,
  * n_conv and max_iters cover the faces that were solved. */
 typedef struct {
@@ -116,7 +119,8 @@ typedef struct {
 
 /* State2D (src/physics/state.py:54-74) as device pointers.
  * cons: D, Sx, Sy, Sz, tau, Bz (state.py:41 EVOLVED_KEYS), double.
- * prims: rho, vx, vy, vz, p, eps, Bx, By, Bz (double, float for HLLD_MIXED). */
+ * prims: rho, vx, vy, vz, p, eps, Bx, By, Bz (double, float for HLLD_MIXED
+ * and HLLD_FP32; in HLLD_FP32 cons, Bxf and Byf are float as well). */
 typedef struct {
     void *cons[6];
     void *Bxf;
@@ -209,14 +213,20 @@ int hlld_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scrat
                     hlld_step_diag_t *diag, void *stream);
 
 /* No counterpart in the reference.  hlld_rk_step_ct for callers that cannot
- * allocate device memory: code running inside CUDA stream capture (cudaMalloc
- * is not allowed there), and hosts whose device memory belongs to a pool or
- * allocator they do not control.  The scratch is a 64 MiB static device
- * array inside the library (held on every GPU that loads it until exit), so
- * grids whose hlld_step2d_scratch_bytes exceeds 64 MiB (square grids above 599^2 cells
- * with ng = 2) get HLLD_ERR_SCRATCH.  Calls that overlap on the GPU share the
- * array and race; the first call on a device looks the array up (make it
- * before any stream capture).  Allocates nothing. */
+ * allocate device memory: hosts whose device memory belongs to a pool or
+ * allocator they do not control (a framework's caching allocator, a
+ * fixed-budget embedded runtime), plugin hosts that hand a solver only its
+ * input and output arrays, and time-step loops that cannot afford the
+ * device-wide synchronisation a cudaMalloc or cudaFree may cause.  The
+ * scratch is a 64 MiB static device array inside the library (held on every
+ * GPU that loads the library until the process exits); grids whose
+ * hlld_step2d_scratch_bytes exceeds 64 MiB get HLLD_ERR_SCRATCH.  With ng = 2
+ * that allows square grids up to 599^2 cells in HLLD_FP64 / HLLD_FP64_EXACT,
+ * 708^2 in HLLD_MIXED and 849^2 in HLLD_FP32.  All calls share the one array
+ * of a device: calls whose work overlaps on the GPU race, so serialise them
+ * on one stream.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress, with that device current) and caches it.
+ * Allocates nothing. */
 int hlld_rk_step_ct_static(const hlld_grid2d_t *g, const hlld_state2d_t *s, double dt_host,
                            const double *dt_dev, int scheme, hlld_step_diag_t *diag,
                            void *stream);
@@ -287,7 +297,7 @@ int hlld_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *cons
  * cell arrays) and F (8 face arrays, slot Bx unused) are work arrays;
  * t_out / steps_out get each tube's final time and step count; next is one
  * device unsigned int (the work counter, zeroed by the call).  Primitives
- * and F are float for HLLD_MIXED, double otherwise. */
+ * and F are float for HLLD_MIXED and HLLD_FP32, double otherwise. */
 int hlld_tubes_run(const hlld_tubes_t *b, void *const *cons, void *const *prims,
                    void *const *U0, void *const *F, double *t_out, int32_t *steps_out,
                    unsigned int *next, int threads, int blocks, void *stream);
