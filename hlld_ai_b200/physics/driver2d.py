@@ -21,6 +21,7 @@ import torch
 from .. import _lib
 from .hlld import flux_diag_from_struct, primitive_to_conserved, solver_name
 from .c2p import conservative_to_primitive
+from .eos import kernel_gamma
 from .state import EVOLVED_KEYS, PRIM_KEYS, State2D, flat, unflat
 
 _SCHEMES = {"rk2": 2, "rk3": 3}
@@ -40,13 +41,17 @@ class Stepper2D:
             raise ValueError(f"unknown boundary condition {(bc_x, bc_y)!r}")
         if limiter not in _lib.LIMITERS:
             raise ValueError(f"unknown limiter {limiter!r}")
-        if precision not in ("fp64", "fp64_exact", "mixed"):
+        if precision not in _lib.PRECISIONS:
             raise ValueError(f"unknown precision {precision!r}")
         self.precision = precision
         # mixed: primitives (and the step's fluxes) are float32; the conserved
-        # state and the staggered field stay float64
-        self.prim_dtype = torch.float32 if precision == "mixed" else torch.float64
+        # state and the staggered field stay float64.  fp32: all float32.
+        self.prim_dtype = torch.float32 if precision in ("mixed", "fp32") else torch.float64
+        self.state_dtype = torch.float32 if precision == "fp32" else torch.float64
         self.grid = grid
+        # the step reads only the grid's sizes and device: this package's
+        # Grid2D and the reference's both qualify
+        self.shape = (grid.nx + 2 * grid.ng, grid.ny + 2 * grid.ng)
         self.device = torch.device(grid.device)
         if self.device.type != "cuda":
             raise TypeError("Grid2D must live on a CUDA device (hlld_ai_b200 has no CPU path)")
@@ -54,7 +59,7 @@ class Stepper2D:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.gc = _lib.Grid2DC(grid.nx, grid.ny, grid.ng, grid.dx, grid.dy, _lib.BCS[bc_x],
                                _lib.BCS[bc_y], _lib.LIMITERS[limiter],
-                               _lib.SOLVERS[solver_name(flux_fn)], eos.kernel_gamma(),
+                               _lib.SOLVERS[solver_name(flux_fn)], kernel_gamma(eos),
                                float(atmo_rho), int(bool(upwind)), _lib.PRECISIONS[precision],
                                _lib.EMF_MODES[emf_mode])
         nbytes = ctypes.c_size_t(0)
@@ -70,15 +75,15 @@ class Stepper2D:
 
     # -- state plumbing ---------------------------------------------------
     def _struct(self, state: State2D) -> _lib.State2DC:
-        g = self.grid
-        cs, fx, fy = (g.nxt, g.nyt), (g.nxt + 1, g.nyt), (g.nxt, g.nyt + 1)
+        nxt, nyt = self.shape
+        cs, fx, fy = (nxt, nyt), (nxt + 1, nyt), (nxt, nyt + 1)
         s = _lib.State2DC()
         for i, k in enumerate(EVOLVED_KEYS):
-            s.cons[i] = self._check(state.cons[k], cs, f"cons[{k!r}]")
+            s.cons[i] = self._check(state.cons[k], cs, f"cons[{k!r}]", self.state_dtype)
         for i, k in enumerate(PRIM_KEYS):
             s.prims[i] = self._check(state.prims[k], cs, f"prims[{k!r}]", self.prim_dtype)
-        s.Bxf = self._check(state.Bxf, fx, "Bxf")
-        s.Byf = self._check(state.Byf, fy, "Byf")
+        s.Bxf = self._check(state.Bxf, fx, "Bxf", self.state_dtype)
+        s.Byf = self._check(state.Byf, fy, "Byf", self.state_dtype)
         return s
 
     def _check(self, t, shape, name, dtype=torch.float64) -> int:
@@ -91,11 +96,10 @@ class Stepper2D:
 
     def ensure_prims(self, state: State2D) -> None:
         """Allocate any primitive array the state lacks (sync fills them)."""
-        g = self.grid
         for k in PRIM_KEYS:
             t = state.prims.get(k)
-            if t is None or not t.is_contiguous() or tuple(t.shape) != (g.nxt, g.nyt):
-                state.prims[k] = torch.zeros(g.nxt, g.nyt, dtype=self.prim_dtype, device=self.device)
+            if t is None or not t.is_contiguous() or tuple(t.shape) != self.shape:
+                state.prims[k] = torch.zeros(self.shape, dtype=self.prim_dtype, device=self.device)
             elif t.dtype != self.prim_dtype:
                 state.prims[k] = t.to(self.prim_dtype).contiguous()
 
@@ -234,10 +238,13 @@ def compute_dt_2d(prims, grid, eos, cfl, speed_of_light=False, precision="fp64")
         return float(cfl / (one / grid.dx + one / grid.dy))
     st = stepper_for(grid, eos, **_opts("outflow", "outflow", "hlld", "mc", "Wv", "solver", True,
                                         1e-10, precision))
-    S = State2D(cons={k: prims["rho"] for k in EVOLVED_KEYS}, Bxf=None, Byf=None, prims=prims)
-    g = grid
-    S.Bxf = torch.empty(g.nxt + 1, g.nyt, dtype=torch.float64, device=st.device)
-    S.Byf = torch.empty(g.nxt, g.nyt + 1, dtype=torch.float64, device=st.device)
+    # the speed kernel reads the primitives only; the other arrays of the
+    # state descriptor are placeholders of the right shapes and types
+    nxt, nyt = st.shape
+    place = torch.empty(nxt, nyt, dtype=st.state_dtype, device=st.device)
+    S = State2D(cons={k: place for k in EVOLVED_KEYS},
+                Bxf=torch.empty(nxt + 1, nyt, dtype=st.state_dtype, device=st.device),
+                Byf=torch.empty(nxt, nyt + 1, dtype=st.state_dtype, device=st.device), prims=prims)
     return float(st.compute_dt(S, cfl).item())
 
 

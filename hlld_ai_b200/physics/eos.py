@@ -18,12 +18,8 @@ class hybrid_eos:
         self.is_cold = gamma_th is None or gamma_th == 1.0
 
     def kernel_gamma(self) -> float:
-        """The adiabatic index the CUDA kernels use; only the ideal-gas EOS
-        of the hot path is implemented on the device."""
-        if self.K != 0 or self.is_cold or self.gamma_th != self.gamma:
-            raise NotImplementedError(
-                "hlld_ai_b200 kernels implement hybrid_eos(K=0, gamma, gamma_th=gamma) only")
-        return float(self.gamma)
+        """The adiabatic index the CUDA kernels use (see ``kernel_gamma``)."""
+        return kernel_gamma(self)
 
     # eos.py:19-76, element-wise on tensors
     def press_cold_eps_cold__rho(self, rho):
@@ -53,3 +49,15 @@ class hybrid_eos:
             press_cold, _ = self.press_cold_eps_cold__rho(rho)
             cs2 = (self.gamma * press_cold + self.gamma_th * (press - press_cold)) / (rho * h)
         return press, cs2
+
+
+def kernel_gamma(eos) -> float:
+    """The adiabatic index of an ideal-gas ``hybrid_eos(K=0, gamma,
+    gamma_th=gamma)``, the only EOS the kernels implement.  Any object with
+    the attributes ``K``, ``gamma`` and ``gamma_th`` is accepted, so the
+    reference's own ``hybrid_eos`` instances drive the step unchanged."""
+    K, gamma, gth = (getattr(eos, a, None) for a in ("K", "gamma", "gamma_th"))
+    if K != 0 or gamma is None or gth is None or gth == 1.0 or gth != gamma:
+        raise NotImplementedError(
+            "hlld_ai_b200 kernels implement hybrid_eos(K=0, gamma, gamma_th=gamma) only")
+    return float(gamma)

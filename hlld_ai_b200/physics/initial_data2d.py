@@ -1,15 +1,26 @@
-"""2D initial conditions, mirroring ``src/physics/initial_data2d.py``.
+"""2D initial conditions of the benchmark and test problems.
 
-Every problem returns cell primitives and a corner vector potential ``Az``;
-the staggered field is its discrete curl (``initial_data2d.py:24-29``), so
-div B is zero to round-off at t = 0.  Tensor arithmetic follows the
-reference on the grid's device (host-side set-up, not the hot path).
+Each problem is a function ``(grid, eos) -> (prims, Az)``: the nine cell
+primitives on the whole ghost-inclusive cell array and the vector potential
+Az at the cell corners.  The staggered field is Az's discrete curl
+(``b_from_potential``), so div B vanishes to round-off at t = 0, which is
+how the reference initialises its CT runs (``initial_data2d.py:24-29``).
+These are host-side set-ups, not part of the hot path.
 
-Beyond the reference's problems:
-  * ``rotor_tapered``: the magnetic rotor on the periodic unit square with a
-    linear density/velocity taper on 0.1 < r < 0.115 (the benchmark rotor);
-  * ``relativistic_vortex``: ``orszag_tang(v_max=0.99, B0=1, press=1, rho=1)``
-    with gamma = 4/3 (the precision-study vortex).
+Problems:
+  * ``rotor``: the magnetic rotor of the reference's ``run_2d.py`` -- a
+    dense disk (r <= 0.1, rho 10, rigid rotation at omega 9.95) in a medium
+    at rest (rho 1), p = 1 and B = (1, 0, 0) everywhere, on [-0.5, 0.5]^2
+    with outflow boundaries;
+  * ``rotor_tapered``: the same rotor centred on the periodic unit square
+    with density and velocity tapered linearly over 0.1 < r < 0.115 (the
+    benchmark rotor);
+  * ``orszag_tang``: v = v_max / sqrt2 (-sin 2 pi y, sin 2 pi x, 0),
+    B = B0 (-sin 2 pi y, sin 4 pi x, 0), uniform rho and p, periodic;
+  * ``vortex``: ``orszag_tang`` with v_max = 0.99, B0 = rho = p = 1,
+    gamma = 4/3 (the precision-study vortex);
+  * ``riemann2d``: the four-quadrant problem of the reference with a uniform
+    in-plane field B0 (cos a, sin a, 0).
 """
 from __future__ import annotations
 
@@ -23,117 +34,101 @@ from .state import EVOLVED_KEYS, State2D
 
 
 def b_from_potential(Az, dx, dy):
-    """initial_data2d.py:24-29"""
-    Bxf = (Az[:, 1:] - Az[:, :-1]) / dy
-    Byf = -(Az[1:, :] - Az[:-1, :]) / dx
-    return Bxf, Byf
+    """Face fields of a corner potential: Bx = d Az / dy on x faces,
+    By = -d Az / dx on y faces (one-cell differences)."""
+    return torch.diff(Az, dim=1) / dy, -torch.diff(Az, dim=0) / dx
 
 
-def _corner_mesh(grid):
-    XF = grid.xf.unsqueeze(1).expand(grid.nxt + 1, grid.nyt + 1)
-    YF = grid.yf.unsqueeze(0).expand(grid.nxt + 1, grid.nyt + 1)
-    return XF, YF
+def _field(grid, value):
+    return torch.full(grid.shape, float(value), dtype=torch.float64, device=grid.device)
+
+
+def _finish(grid, eos, rho, p, v, B):
+    """The nine primitives from density, pressure, velocity and field."""
+    prims = {"rho": rho, "p": p, "vx": v[0], "vy": v[1], "vz": v[2],
+             "Bx": B[0], "By": B[1], "Bz": B[2]}
+    for k, t in prims.items():
+        if not isinstance(t, torch.Tensor):
+            prims[k] = _field(grid, t)
+    prims["eps"] = eos.eps__press_rho(prims["p"], prims["rho"])
+    return prims
 
 
 def magnetic_rotor(grid, eos, r0=0.1, rho_in=10.0, rho_out=1.0, omega=9.95, press=1.0, B0=1.0):
-    """initial_data2d.py:88-125: sharp-edged rotor on [-0.5, 0.5]^2."""
+    """The rotor of the reference's ``run_2d.py`` problem table, on a grid
+    centred on the origin: a sharp disk edge at r0 (cells whose centres lie
+    within r0, allowing 16 ulp for the radius of a centre exactly on it)."""
     X, Y = grid.X, grid.Y
-    r2 = X**2 + Y**2
-    inside = r2 <= r0 * r0 * (1.0 + 16 * torch.finfo(torch.float64).eps)
-    zeros = torch.zeros(grid.shape, dtype=torch.float64, device=grid.device)
-    prims = {
-        "rho": torch.where(inside, torch.full_like(zeros, rho_in), torch.full_like(zeros, rho_out)),
-        "p": torch.full_like(zeros, press),
-        "vx": torch.where(inside, -omega * Y, zeros),
-        "vy": torch.where(inside, omega * X, zeros),
-        "vz": zeros.clone(),
-        "Bx": torch.full_like(zeros, B0),
-        "By": zeros.clone(),
-        "Bz": zeros.clone(),
-    }
-    prims["eps"] = eos.eps__press_rho(prims["p"], prims["rho"])
-    _, YF = _corner_mesh(grid)
-    return prims, B0 * YF
+    inside = X * X + Y * Y <= r0 * r0 * (1.0 + 16.0 * 2.0 ** -52)
+    zero = _field(grid, 0.0)
+    rho = torch.where(inside, _field(grid, rho_in), _field(grid, rho_out))
+    v = (torch.where(inside, -omega * Y, zero), torch.where(inside, omega * X, zero), zero.clone())
+    _, yc = grid.corner_mesh()
+    return _finish(grid, eos, rho, press, v, (B0, 0.0, 0.0)), B0 * yc
 
 
 def rotor_tapered(grid, eos, r0=0.1, r1=0.115, rho_in=10.0, rho_out=1.0, omega=9.95,
                   press=1.0, B0=1.0, centre=(0.5, 0.5)):
-    """Benchmark rotor: disk r <= r0 (rho_in, rigid rotation omega) inside an
-    ambient medium (rho_out, at rest), both tapered linearly in f = (r1 - r) /
-    (r1 - r0) on r0 < r < r1; uniform p and B = (B0, 0, 0) (Az = B0 y)."""
+    """The benchmark rotor: the disk r <= r0 at `centre`, its density and
+    angular velocity falling linearly to the ambient values over r0 < r < r1."""
     X = grid.X - centre[0]
     Y = grid.Y - centre[1]
-    r = torch.sqrt(X**2 + Y**2)
-    f = torch.clamp((r1 - r) / (r1 - r0), min=0.0, max=1.0)
-    zeros = torch.zeros(grid.shape, dtype=torch.float64, device=grid.device)
-    prims = {
-        "rho": rho_out + (rho_in - rho_out) * f,
-        "p": torch.full_like(zeros, press),
-        "vx": -omega * Y * f,
-        "vy": omega * X * f,
-        "vz": zeros.clone(),
-        "Bx": torch.full_like(zeros, B0),
-        "By": zeros.clone(),
-        "Bz": zeros.clone(),
-    }
-    prims["eps"] = eos.eps__press_rho(prims["p"], prims["rho"])
-    _, YF = _corner_mesh(grid)
-    return prims, B0 * YF
+    f = ((r1 - torch.sqrt(X * X + Y * Y)) / (r1 - r0)).clamp(0.0, 1.0)
+    rho = rho_out + (rho_in - rho_out) * f
+    v = (-omega * Y * f, omega * X * f, _field(grid, 0.0))
+    _, yc = grid.corner_mesh()
+    return _finish(grid, eos, rho, press, v, (B0, 0.0, 0.0)), B0 * yc
 
 
 def riemann2d(grid, eos, B0=0.5, angle_deg=45.0, angle_z_deg=0.0):
-    """initial_data2d.py:128-191: four-quadrant problem with a uniform field."""
-    X, Y = grid.X, grid.Y
-    zeros = torch.zeros(grid.shape, dtype=torch.float64, device=grid.device)
-    right, top = X > 0.0, Y > 0.0
-    full = lambda v: torch.full_like(zeros, float(v))
-
-    def pick(tl, tr, bl, br):
-        return torch.where(top, torch.where(right, full(tr), full(tl)),
-                           torch.where(right, full(br), full(bl)))
-
+    """Four constant quadrants on [-0.5, 0.5]^2, (rho, p, vx, vy) =
+    top left (0.1, 1, 0.99, 0), top right (0.1, 0.01, 0, 0), bottom left
+    (0.5, 1, 0, 0), bottom right (0.1, 1, 0, 0.99), in the uniform field
+    B0 (cos a cos b, sin a cos b, sin b); at a = 45 degrees the in-plane
+    components are set equal, so the problem keeps its x <-> y symmetry."""
     a, b = math.radians(angle_deg), math.radians(angle_z_deg)
-    ca, sa = math.cos(a), math.sin(a)
-    if angle_deg == 45.0:
-        sa = ca
+    ca = math.cos(a)
+    sa = ca if angle_deg == 45.0 else math.sin(a)
     bx, by, bz = B0 * ca * math.cos(b), B0 * sa * math.cos(b), B0 * math.sin(b)
-    prims = {"rho": pick(0.1, 0.1, 0.5, 0.1), "p": pick(1.0, 0.01, 1.0, 1.0),
-             "vx": pick(0.99, 0.0, 0.0, 0.0), "vy": pick(0.0, 0.0, 0.0, 0.99),
-             "vz": zeros.clone(), "Bx": full(bx), "By": full(by), "Bz": full(bz)}
-    prims["eps"] = eos.eps__press_rho(prims["p"], prims["rho"])
-    XF, YF = _corner_mesh(grid)
-    return prims, bx * YF - by * XF
+    east, north = grid.X > 0.0, grid.Y > 0.0
+
+    def quadrants(nw, ne, sw, se):
+        row_n = torch.where(east, _field(grid, ne), _field(grid, nw))
+        row_s = torch.where(east, _field(grid, se), _field(grid, sw))
+        return torch.where(north, row_n, row_s)
+
+    prims = _finish(grid, eos, quadrants(0.1, 0.1, 0.5, 0.1), quadrants(1.0, 0.01, 1.0, 1.0),
+                    (quadrants(0.99, 0.0, 0.0, 0.0), quadrants(0.0, 0.0, 0.0, 0.99), 0.0),
+                    (bx, by, bz))
+    xc, yc = grid.corner_mesh()
+    return prims, bx * yc - by * xc
 
 
 def orszag_tang(grid, eos, v_max=0.99, B0=None, press=None, rho=None):
-    """initial_data2d.py:194-253"""
-    if B0 is None:
-        B0 = 1.0 / math.sqrt(4.0 * math.pi)
-    if rho is None:
-        rho = 25.0 / (36.0 * math.pi)
-    if press is None:
-        press = 5.0 / (12.0 * math.pi)
+    """The relativistic Orszag-Tang vortex on the periodic unit square.  The
+    defaults B0 = 1/sqrt(4 pi), rho = 25/(36 pi), p = 5/(12 pi) are the
+    classical vortex's; the field's potential is
+    Az = B0 (cos 4 pi x / (4 pi) + cos 2 pi y / (2 pi))."""
+    B0 = 1.0 / math.sqrt(4.0 * math.pi) if B0 is None else B0
+    rho = 25.0 / (36.0 * math.pi) if rho is None else rho
+    press = 5.0 / (12.0 * math.pi) if press is None else press
+    k = 2.0 * math.pi
+    sx, sy = torch.sin(k * grid.X), torch.sin(k * grid.Y)
     amp = v_max / math.sqrt(2.0)
-    X, Y = grid.X, grid.Y
-    zeros = torch.zeros(grid.shape, dtype=torch.float64, device=grid.device)
-    prims = {"rho": torch.full_like(zeros, rho), "p": torch.full_like(zeros, press),
-             "vx": -amp * torch.sin(2 * math.pi * Y), "vy": amp * torch.sin(2 * math.pi * X),
-             "vz": zeros.clone(), "Bx": -B0 * torch.sin(2 * math.pi * Y),
-             "By": B0 * torch.sin(4 * math.pi * X), "Bz": zeros.clone()}
-    prims["eps"] = eos.eps__press_rho(prims["p"], prims["rho"])
-    XF, YF = _corner_mesh(grid)
-    Az = B0 * (torch.cos(4 * math.pi * XF) / (4 * math.pi) + torch.cos(2 * math.pi * YF) / (2 * math.pi))
+    prims = _finish(grid, eos, rho, press, (-amp * sy, amp * sx, 0.0),
+                    (-B0 * sy, B0 * torch.sin(2.0 * k * grid.X), 0.0))
+    xc, yc = grid.corner_mesh()
+    Az = B0 * (torch.cos(2.0 * k * xc) / (2.0 * k) + torch.cos(k * yc) / k)
     return prims, Az
 
 
 def relativistic_vortex(grid, eos):
-    """Precision-study vortex: v = 0.99/sqrt2 (-sin 2pi y, sin 2pi x, 0),
-    B = (-sin 2pi y, sin 4pi x, 0), rho = p = 1 (use gamma = 4/3)."""
+    """The precision-study vortex (use gamma = 4/3)."""
     return orszag_tang(grid, eos, v_max=0.99, B0=1.0, press=1.0, rho=1.0)
 
 
-# problem -> (domain, gamma, t_end, (bc_x, bc_y), builder); the first four
-# follow scripts/run_2d.py:30-41
+# problem -> domain, adiabatic index, end time, boundaries (x, y), builder;
+# the first three are the reference run_2d.py's set-ups
 PROBLEMS = {
     "rotor": dict(box=(-0.5, 0.5), gamma=5.0 / 3.0, tend=0.4, bc=("outflow", "outflow"),
                   build=magnetic_rotor),
@@ -149,7 +144,7 @@ PROBLEMS = {
 
 
 def initial_prims(problem: str, n: int, ng: int = 2, device="cpu"):
-    """(grid, eos, prims, Az, spec) of a named problem, built on `device`."""
+    """(grid, eos, prims, Az, spec) of a named problem on an n x n grid."""
     spec = PROBLEMS[problem]
     lo, hi = spec["box"]
     g = Grid2D(lo, hi, n, lo, hi, n, ng=ng, device=device)
@@ -162,9 +157,10 @@ def setup_problem(problem: str, n: int, *, limiter: str = "mc", device="cuda",
                   precision: str = "fp64"):
     """A synced GPU State2D of a named problem: (grid, eos, state, spec).
 
-    Initial data are built on the CPU with the reference's tensor formulas,
-    moved to the device, converted to conserved variables and synced there
-    (scripts/run_2d.py:216-231)."""
+    The primitives and the potential are evaluated on the CPU, the staggered
+    field and the conserved variables are formed on the device (in FP64 for
+    every precision), then stored in the precision's types and synced, so
+    that the primitives the step starts from are the C2P of its own state."""
     from ..physics.reconstruction import ghosts_needed
     from .driver2d import prims_to_cons_2d, sync_state
 
@@ -173,10 +169,12 @@ def setup_problem(problem: str, n: int, *, limiter: str = "mc", device="cuda",
     g = Grid2D(gc.xmin, gc.xmax, n, gc.ymin, gc.ymax, n, ng=ng, device=device)
     prims = {k: v.contiguous().to(device) for k, v in prims.items()}
     Bxf, Byf = b_from_potential(Az.to(device), g.dx, g.dy)
-    # conserved variables from the FP64 initial primitives in every precision
     c = prims_to_cons_2d(prims, g, "fp64_exact" if precision == "fp64_exact" else "fp64")
-    if precision == "mixed":
+    if precision in ("mixed", "fp32"):
         prims = {k: v.to(torch.float32).contiguous() for k, v in prims.items()}
+    if precision == "fp32":
+        c = {k: v.to(torch.float32) for k, v in c.items()}
+        Bxf, Byf = Bxf.to(torch.float32), Byf.to(torch.float32)
     st = State2D(cons={k: c[k].contiguous() for k in EVOLVED_KEYS}, Bxf=Bxf.contiguous(),
                  Byf=Byf.contiguous(), prims=prims)
     st = sync_state(st, g, eos, *spec["bc"], precision=precision, limiter=limiter)

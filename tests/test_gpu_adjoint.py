@@ -39,7 +39,7 @@ def smooth_random_state(n, limiter="mc", seed=1, solver="hlld", upwind=True, sch
     random-phase sinusoids, B from a random potential plus a uniform part."""
     from hlld_ai_b200.physics.driver2d import prims_to_cons_2d
     from hlld_ai_b200.physics.grid import Grid2D
-    from hlld_ai_b200.physics.initial_data2d import _corner_mesh, b_from_potential
+    from hlld_ai_b200.physics.initial_data2d import b_from_potential
     from hlld_ai_b200.physics.reconstruction import ghosts_needed
 
     eos = H.hybrid_eos(K=0.0, gamma=5.0 / 3.0, gamma_th=5.0 / 3.0)
@@ -58,7 +58,7 @@ def smooth_random_state(n, limiter="mc", seed=1, solver="hlld", upwind=True, sch
     prims = {"rho": 1.0 + 0.3 * field(X, Y), "p": 1.0 + 0.3 * field(X, Y),
              "vx": 0.3 * field(X, Y), "vy": 0.3 * field(X, Y), "vz": 0.2 * field(X, Y),
              "Bz": 0.4 * field(X, Y)}
-    XF, YF = _corner_mesh(g)
+    XF, YF = g.corner_mesh()
     Az = 0.5 * YF - 0.3 * XF + 0.05 * field(XF, YF)
     Bxf, Byf = b_from_potential(Az, g.dx, g.dy)
     Bxf, Byf = Bxf.contiguous(), Byf.contiguous()

@@ -227,3 +227,25 @@ def test_step_rejects_bad_state():
                   prims=st.prims)
     with pytest.raises(TypeError):
         stepper.step(cpu, 1e-3)
+
+
+def test_stepper_takes_reference_shaped_grid_and_eos():
+    """A caller inside the reference passes its own Grid2D and hybrid_eos:
+    the stepper reads only nx, ny, ng, dx, dy, device and K, gamma,
+    gamma_th, so objects with just those attributes give the same step."""
+    from types import SimpleNamespace
+
+    g, eos, st, stepper, og, ostate = build("rotor_tapered", 48, 40, "mc", "hlld", "fp64")
+    ref_grid = SimpleNamespace(nx=g.nx, ny=g.ny, ng=g.ng, dx=g.dx, dy=g.dy, device=g.device,
+                               nxt=g.nxt, nyt=g.nyt)
+    ref_eos = SimpleNamespace(K=0.0, gamma=eos.gamma, gamma_th=eos.gamma)
+    other = H.Stepper2D(ref_grid, ref_eos, bc_x="periodic", bc_y="periodic", flux_fn="hlld",
+                        limiter="mc", precision="fp64")
+    twin = st.clone()
+    for _ in range(2):
+        dt = stepper.compute_dt(st, 0.4)
+        stepper.step(st, dt, "rk3")
+        other.step(twin, dt, "rk3")
+    for k in EVOLVED_KEYS:
+        assert bitwise_equal(st.cons[k].cpu().numpy(), twin.cons[k].cpu().numpy()), k
+    assert bitwise_equal(st.Byf.cpu().numpy(), twin.Byf.cpu().numpy())
