@@ -2,19 +2,20 @@
 // fixed device array that is part of the library, for callers that cannot
 // allocate device memory themselves.
 //
-// Who cannot allocate: code that runs while a CUDA stream is being captured
-// into a graph (cudaMalloc/cudaFree are not allowed in global capture mode
-// and synchronise the device otherwise), hosts whose device memory belongs to
-// a pool or allocator they do not control (a framework's caching allocator, a
-// fixed-budget embedded runtime), and plugin hosts that hand a solver only its
-// input and output arrays.  For them the scratch (face fluxes, corner EMF,
-// the RK stage-0 copy, counters) lives in g_step_scratch below.
+// Who cannot allocate: hosts whose device memory belongs to a pool or
+// allocator they do not control (a framework's caching allocator, a
+// fixed-budget embedded runtime), plugin hosts that hand a solver only its
+// input and output arrays, and time-step loops that cannot afford the
+// device-wide synchronisation a cudaMalloc or cudaFree may cause.  For them
+// the scratch (face fluxes, corner EMF, the RK stage-0 copy, counters and,
+// in the mixed form, the C2P roots of the first stage) lives in
+// g_step_scratch below.
 //
 // Limits and rules:
 //   - the array holds kStaticScratchBytes (64 MiB); hlld_step2d_scratch_bytes
-//     says what a grid needs (about 23 x 8 B x (nx+2ng+1)(ny+2ng+1), i.e.
-//     square grids up to 599 x 599 cells with ng = 2); larger grids get
-//     HLLD_ERR_SCRATCH;
+//     says what a grid needs; with ng = 2 that is square grids up to
+//     599 x 599 cells in FP64, 708 x 708 in the mixed form and 849 x 849 in
+//     FP32; larger grids get HLLD_ERR_SCRATCH;
 //   - every GPU that loads the library keeps the 64 MiB until the process
 //     exits;
 //   - all calls share the one array per device, so calls whose work overlaps
@@ -23,8 +24,7 @@
 //     the array before reading it, so leftover contents of an earlier call are
 //     harmless;
 //   - the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before any stream capture begins.
+//     (cudaGetSymbolAddress, with that device current) and caches it.
 #include <cstdio>
 #include <mutex>
 
