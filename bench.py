@@ -19,9 +19,24 @@ N > 1 (torchrun): every rank advances its own rotor replica (the reference
 path has no domain decomposition; replicas only) and the rate is the sum
 over ranks timed by the slowest rank.
 
+The default line also carries, each in its own block:
+  * ``fp64``: the FP64 step's rate, its share of faces without normal field
+    and the 20-step density L1/Linf of the mixed run against it;
+  * ``later_state``: both forms timed from the rotor at t = 0.2 (advanced
+    untimed in the mixed form, then loaded into both);
+  * ``fp32``: the all-FP32 step's rate and its 20-step density L1/Linf
+    against FP64 at n^2 and (n/2)^2;
+  * ``vortex``: the relativistic vortex (gamma 4/3) -- mixed and FP64 rates
+    at n^2 and the L1/Linf of rho, p, |B|^2 at t = 0.5 at --vortex-n^2 of
+    the mixed run and of a 1e-13-perturbed FP64 run against FP64;
+  * ``tubes``: 4096 seeded tubes, mixed and FP64 cell-updates/s, the tube
+    kernel's roofline, and the density L1 against the oracle of a seeded
+    subset advanced to t = 0.3;
+  * ``adjoint``: the rotor gradient study's adjoint/forward cost.
+
 ``--impl reference`` times the CPU oracle (a C restatement of the
 reference's FP64 path) on the host cores with all threads, one RK3 step of
-the same rotor at 512^2 per step as a bounded sample.
+the same rotor at 1024^2 (``--cpu-n``) per step as a bounded sample.
 """
 from __future__ import annotations
 
@@ -70,6 +85,15 @@ def parse():
     ap.add_argument("--chunk", type=float, default=0.01,
                     help="tubes: simulated time every tube advances per step")
     ap.add_argument("--cpu-tubes", type=int, default=30, help="tubes of the CPU baseline sample")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the later_state, fp32, vortex and tubes blocks of the default line")
+    ap.add_argument("--t-later", type=float, default=0.2, help="rotor time of the later_state block")
+    ap.add_argument("--vortex-n", type=int, default=1024,
+                    help="grid of the vortex block's t = 0.5 precision study")
+    ap.add_argument("--vortex-tend", type=float, default=0.5)
+    ap.add_argument("--tube-check", type=int, default=30,
+                    help="seeded tubes of the tube block's accuracy check against the oracle")
+    ap.add_argument("--tube-tend", type=float, default=0.3)
     return ap.parse_args()
 
 
@@ -322,15 +346,23 @@ def _l1_mixed_vs_fp64(a, dev, steps):
 
 
 # DRAM bytes (read + write) of one mixed-precision sweep launch measured by
-# ncu on the rotor at 1536^2 (x: 95.0 + 79.4 MB, y: 95.5 + 54.2 MB over
-# 2,373,140 faces), per face; the 2048^2 launch is scaled by its faces
-_SWEEP_DRAM_BYTES_PER_FACE_MIXED = (174.3e6 + 149.7e6) / 2 / 2373140
+# ncu on the rotor at 1536^2 (x: 95.44 + 74.61 MB, y: 95.87 + 51.18 MB over
+# 2,373,140 faces each; profiles/sweep_kernel_rotor1536_mixed_ncu.md), per
+# face; the 2048^2 launch is scaled by its faces
+_SWEEP_DRAM_BYTES_PER_FACE_MIXED = (170.05e6 + 147.05e6) / 2 / 2373140
+# FP64-pipe instructions (warp level) of the same two launches, per face
+_SWEEP_FP64_INST_PER_FACE_MIXED = (126.13e6 + 10.01e6) / 2 / 2373140
+# FP64 issue rate of one B200 SM: 2 warp instructions per cycle (64 lanes;
+# the ncu capture's 126.1 M FP64 instructions at 35.0 % of peak sustained
+# over 637 us at 1965 MHz on 148 SMs give 1.94)
+_FP64_WARP_INST_PER_SM_CYCLE = 2
 
 
 # DRAM bytes (read + write) of one mixed-precision tubes_kernel launch
-# measured by ncu (2048 seeded tubes, chunk 0.0005: 8.05 + 11.53 GB over
-# 2.129e7 cell-updates), per cell-update; a launch is scaled by its updates
-_TUBES_DRAM_BYTES_PER_UPDATE_MIXED = (8.053e9 + 11.526e9) / 2.129e7
+# measured by ncu (2048 seeded tubes, chunk 0.0005: 6.046 + 8.150 GB over
+# 2.129e7 cell-updates; profiles/tubes_kernel_2048tubes_ncu.md), per
+# cell-update; a launch is scaled by its updates
+_TUBES_DRAM_BYTES_PER_UPDATE_MIXED = (6.046e9 + 8.150e9) / 2.129e7
 
 
 def _sweep_traffic(a):
@@ -338,6 +370,261 @@ def _sweep_traffic(a):
         return None
     nt = a.n + 4
     return _SWEEP_DRAM_BYTES_PER_FACE_MIXED * (nt + 1) * nt
+
+
+def _time_public(stepper, st, steps, warmup, cfl, rp):
+    """Mean ms per step of the on-device CFL dt + one RK3 step through the
+    public Stepper2D, after `warmup` steps (CUDA events on the current
+    stream, the slowest rank's time); also the share of faces without normal
+    field in the last stage's x and y sweeps."""
+    import torch
+
+    from hlld_ai_b200 import _lib, replicas
+
+    dev = stepper.device
+    for _ in range(warmup):
+        stepper.step(st, stepper.compute_dt(st, cfl), "rk3")
+    torch.cuda.synchronize(dev)
+    replicas.barrier(rp)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        stepper.step(st, stepper.compute_dt(st, cfl), "rk3")
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    (ms,) = replicas.max_over_ranks(rp, e0.elapsed_time(e1))
+    d = _lib.StepDiag.from_buffer_copy(stepper.diag_buf.cpu().numpy().tobytes())
+    bn0 = [d.sweep[k].n_bn_zero / max(d.sweep[k].n_faces, 1) for k in (0, 1)]
+    return ms / steps, bn0
+
+
+def _stepper(problem, n, precision, dev):
+    import hlld_ai_b200 as H
+
+    g, eos, st, spec = H.setup_problem(problem, n, limiter="mc", device=dev, precision=precision)
+    stp = H.Stepper2D(g, eos, bc_x=spec["bc"][0], bc_y=spec["bc"][1], flux_fn="hlld",
+                      limiter="mc", precision=precision)
+    return g, st, stp
+
+
+def _l1_vs_fp64(a, dev, steps, n, precision):
+    """Density L1 / Linf (mean / max |rho - rho_fp64| over physical cells) of
+    `precision` against FP64 after `steps` RK3 steps of the rotor from the
+    same initial state with the FP64 run's dt, and the C2P and fallback
+    counters of the last step."""
+    import torch
+
+    runs = {p: _stepper(PROBLEM, n, p, dev) for p in ("fp64", precision)}
+    for _ in range(steps):
+        dt = float(runs["fp64"][2].compute_dt(runs["fp64"][1], a.cfl).item())
+        for p in runs:
+            runs[p][2].step(runs[p][1], dt, "rk3")
+    g = runs["fp64"][0]
+    r64 = runs["fp64"][1].prims["rho"][g.phys]
+    d = (runs[precision][1].prims["rho"][g.phys].double() - r64).abs()
+    diag = runs[precision][2].diag()
+    out = {"n": n, "steps": steps, "l1_rho": float(d.mean()), "linf_rho": float(d.max()),
+           "l1_rho_rel": float(d.mean() / r64.abs().mean()),
+           "c2p_not_converged": diag["c2p"]["not_converged"], "c2p_atmo": diag["c2p"]["atmo"],
+           "hlle_fallback_frac": {"x": diag["x"]["diag"]["frac_hlle_fallback"],
+                                  "y": diag["y"]["diag"]["frac_hlle_fallback"]}}
+    del runs
+    torch.cuda.empty_cache()
+    return out
+
+
+def _later_state_block(a, rp, dev):
+    """Both forms timed from the rotor at t = a.t_later: the mixed run is
+    advanced there untimed, its FP64 conserved state and staggered field are
+    loaded into an FP64 stepper, then each form is timed a.steps steps."""
+    import torch
+
+    from hlld_ai_b200.physics.state import EVOLVED_KEYS, State2D
+
+    g, st, stp = _stepper(PROBLEM, a.n, "mixed", dev)
+    t, nsteps = 0.0, 0
+    while t < a.t_later:
+        dt = stp.compute_dt(st, a.cfl)
+        stp.step(st, dt, "rk3")
+        t += float(dt.item())
+        nsteps += 1
+    snap = State2D(cons={k: st.cons[k].clone() for k in EVOLVED_KEYS}, Bxf=st.Bxf.clone(),
+                   Byf=st.Byf.clone(), prims={})
+    ms_mx, bn_mx = _time_public(stp, st, a.steps, a.warmup, a.cfl, rp)
+    del st, stp
+    torch.cuda.empty_cache()
+    g64, st64, stp64 = _stepper(PROBLEM, a.n, "fp64", dev)
+    del st64
+    stp64.sync(snap)
+    ms_64, bn_64 = _time_public(stp64, snap, a.steps, a.warmup, a.cfl, rp)
+    del snap, stp64
+    torch.cuda.empty_cache()
+    zones = a.n * a.n * rp.world
+    return {"t": t, "steps_to_reach": nsteps,
+            "mixed": {"ms_per_step": ms_mx, "value": zones / (ms_mx * 1e-3),
+                      "bn_zero_face_share": {"x": bn_mx[0], "y": bn_mx[1]}},
+            "fp64": {"ms_per_step": ms_64, "value": zones / (ms_64 * 1e-3),
+                     "bn_zero_face_share": {"x": bn_64[0], "y": bn_64[1]}},
+            "mixed_speedup": ms_64 / ms_mx,
+            "note": "both forms from the same state at t (the mixed run's), each timed through "
+                    "Stepper2D.step + compute_dt"}
+
+
+def _fp32_block(a, rp, dev):
+    import torch
+
+    g, st, stp = _stepper(PROBLEM, a.n, "fp32", dev)
+    ms, bn0 = _time_public(stp, st, a.steps, a.warmup, a.cfl, rp)
+    del st, stp
+    torch.cuda.empty_cache()
+    zones = a.n * a.n * rp.world
+    return {"ms_per_step": ms, "value": zones / (ms * 1e-3),
+            "bn_zero_face_share": {"x": bn0[0], "y": bn0[1]},
+            "vs_fp64": [_l1_vs_fp64(a, dev, 20, n, "fp32") for n in (a.n, a.n // 2)]}
+
+
+def _vortex_block(a, rp, dev):
+    """Config 3: the relativistic vortex.  Rates of the mixed and FP64 steps
+    at a.n^2; at a.vortex_n^2 to t = a.vortex_tend the L1 / Linf of rho, p
+    and |B|^2 of the mixed run and of an FP64 run whose initial D and tau
+    carry 1e-13 relative noise, both against FP64 (same dt sequence)."""
+    import torch
+
+    zones = a.n * a.n * rp.world
+    rates = {}
+    for prec in ("mixed", "fp64"):
+        g, st, stp = _stepper("vortex", a.n, prec, dev)
+        ms, _ = _time_public(stp, st, max(5, a.steps // 2), a.warmup, a.cfl, rp)
+        rates[prec] = {"ms_per_step": ms, "value": zones / (ms * 1e-3)}
+        del st, stp
+        torch.cuda.empty_cache()
+    n = a.vortex_n
+    runs = {p: _stepper("vortex", n, p, dev) for p in ("fp64", "mixed")}
+    g, pert, sp = _stepper("vortex", n, "fp64", dev)
+    gen = torch.Generator(device=dev).manual_seed(1)
+    for k in ("D", "tau"):
+        noise = 2 * torch.rand(pert.cons[k].shape, generator=gen, device=dev, dtype=torch.float64) - 1
+        pert.cons[k].mul_(1 + 1e-13 * noise)
+    sp.sync(pert)
+    t, steps = 0.0, 0
+    while t < a.vortex_tend - 1e-14:
+        dt = min(float(runs["fp64"][2].compute_dt(runs["fp64"][1], a.cfl).item()), a.vortex_tend - t)
+        for p in runs:
+            runs[p][2].step(runs[p][1], dt, "rk3")
+        sp.step(pert, dt, "rk3")
+        t += dt
+        steps += 1
+    ph = g.phys
+    fields = {"rho": lambda P: P["rho"][ph].double(), "p": lambda P: P["p"][ph].double(),
+              "B2": lambda P: sum(P[k][ph].double() ** 2 for k in ("Bx", "By", "Bz"))}
+    ref = runs["fp64"][1].prims
+
+    def norms(P):
+        out = {}
+        for name, f in fields.items():
+            d = (f(P) - f(ref)).abs()
+            out[name] = {"l1": float(d.mean()), "linf": float(d.max())}
+        return out
+
+    res = {"n_rates": a.n, "mixed": rates["mixed"], "fp64": rates["fp64"],
+           "mixed_speedup": rates["fp64"]["ms_per_step"] / rates["mixed"]["ms_per_step"],
+           "study": {"n": n, "t": t, "steps": steps,
+                     "mixed_vs_fp64": norms(runs["mixed"][1].prims),
+                     "fp64_perturbed_1e-13_vs_fp64": norms(pert.prims)}}
+    del runs, pert, sp
+    torch.cuda.empty_cache()
+    return res
+
+
+def _oracle_tubes(states, idx, tend, threads):
+    """Primitives of tubes `idx` advanced to tend by the oracle (one tube per
+    host thread; the C call releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle
+    from hlld_ai_b200.tubes import tube_prims
+
+    def one(i):
+        p = tube_prims(states, i, 3)
+        L = int(states.lengths[i])
+        oracle.tube_run(p, L, 3, 1.0 / L, 0.4, tend, "weno5z", "hlld", 5.0 / 3.0)
+        return p
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        return list(ex.map(one, idx))
+
+
+def _tubes_block(a, rp, dev):
+    """Config 4: 4096 seeded tubes.  Mixed and FP64 cell-updates/s (graph
+    replays advancing every tube by a.chunk) and the L1 of rho against the
+    oracle on a seeded subset of a.tube_check tubes advanced to a.tube_tend."""
+    import numpy as np
+    import torch
+
+    from hlld_ai_b200 import replicas
+    from hlld_ai_b200.tubes import TubeBatch, TubeStates, random_tubes
+
+    states = random_tubes(a.tubes, seed=replicas.replica_seed(20261203, rp))
+    L = torch.as_tensor(states.lengths, dtype=torch.int64, device=dev)
+    peak, kind = peaks()
+    out = {"workload": TUBES_WORKLOAD, "tubes": a.tubes, "chunk": a.chunk}
+    for prec in ("mixed", "fp64"):
+        b = TubeBatch(states, limiter="weno5z", solver="hlld", scheme="rk3", precision=prec,
+                      device=dev)
+        tuned = b.autotune(tend=a.chunk / 4, sample=512)
+        g = b.capture(tend=a.chunk)
+        b.reset()
+        g.replay()  # warm-up
+        torch.cuda.synchronize(dev)
+        reps = 3 if prec == "mixed" else 2
+        stream = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        acc = torch.zeros(a.tubes, dtype=torch.int64, device=dev)
+        e0.record(stream)
+        for _ in range(reps):
+            g.replay()
+            acc += b.steps_out
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        (ms,) = replicas.max_over_ranks(rp, e0.elapsed_time(e1))
+        (updates,) = replicas.sum_over_ranks(rp, float((acc * L).sum().item()))
+        rb = 4 if prec == "mixed" else 8
+        per_launch = updates / rp.world / reps
+        bytes_per_update = 3 * (14 * rb + 14 * 8) + 2 * 7 * 8
+        achieved = bytes_per_update * per_launch / (ms / reps * 1e-3) / 1e9
+        out[prec] = {"value": updates / (ms * 1e-3), "unit": "cell-updates/s",
+                     "ms_per_launch": ms / reps, "threads": tuned[0], "blocks": tuned[1],
+                     "roofline": {"bound": "hbm", "achieved": achieved, "unit": "GB/s",
+                                  "peak": peak, "peak_kind": kind, "frac": achieved / peak,
+                                  "bytes_per_cell_update": bytes_per_update}}
+        del b, g
+        torch.cuda.empty_cache()
+    out["mixed"]["roofline"]["traffic_per_cell_update"] = _TUBES_DRAM_BYTES_PER_UPDATE_MIXED
+    out["mixed"]["roofline"]["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                                  "of the mixed launch on 2048 tubes")
+    out["mixed_speedup"] = out["mixed"]["value"] / out["fp64"]["value"]
+    # accuracy: a seeded subset to t = a.tube_tend against the oracle
+    rng = np.random.default_rng(7)
+    idx = sorted(rng.choice(a.tubes, size=min(a.tube_check, a.tubes), replace=False).tolist())
+    sub = TubeStates(states.lengths[idx], {k: v[idx] for k, v in states.left.items()},
+                     {k: v[idx] for k, v in states.right.items()}, states.Bx[idx])
+    ref = _oracle_tubes(sub, list(range(len(idx))), a.tube_tend, os.cpu_count() or 1)
+    check = {"tubes": len(idx), "t": a.tube_tend, "seed": 7}
+    for prec in ("mixed", "fp64"):
+        b = TubeBatch(sub, limiter="weno5z", solver="hlld", scheme="rk3", precision=prec,
+                      device=dev)
+        b.launch(tend=a.tube_tend)
+        torch.cuda.synchronize(dev)
+        errs = []
+        for i in range(len(idx)):
+            got, want = b.tube(i)["rho"][3:-3], ref[i]["rho"][3:-3]
+            errs.append(float(np.abs(got - want).mean() / np.abs(want).mean()))
+        check[prec] = {"l1_rho_rel_median": float(np.median(errs)),
+                       "l1_rho_rel_max": float(np.max(errs))}
+        del b
+    out["vs_oracle"] = check
+    return out
 
 
 def run_ours(a):
@@ -371,6 +658,20 @@ def run_ours(a):
     achieved = bytes_per_face * main["faces"] / sweep_avg_s / 1e9
     peak, peak_kind = peaks()
     sweep_share = sum(sweep_ms) / ms
+    # the compute side: FP64-pipe instructions per launch (ncu, scaled by
+    # faces) over the launch time, against the SMs' FP64 issue rate at the
+    # median SM clock sampled during the timed region
+    fp64_pipe = None
+    if a.precision == "mixed" and clk and clk.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        inst = _SWEEP_FP64_INST_PER_FACE_MIXED * main["faces"]
+        rate = inst / sweep_avg_s
+        peak_rate = sms * _FP64_WARP_INST_PER_SM_CYCLE * clk["sm_mhz"] * 1e6
+        fp64_pipe = {"inst_per_launch": inst, "achieved_inst_per_s": rate,
+                     "peak_inst_per_s": peak_rate, "frac": rate / peak_rate,
+                     "source": "ncu sm__inst_executed_pipe_fp64.sum of the mixed sweeps at "
+                               "1536^2 scaled by faces; peak 2 FP64 warp instructions per SM "
+                               "cycle at the sampled SM clock"}
 
     fp64_arm = None
     if a.precision == "mixed" and not a.no_fp64_arm:
@@ -378,7 +679,9 @@ def run_ours(a):
         torch.cuda.empty_cache()
         r64 = _timed_rotor(a, "fp64", rp, record=False)
         fp64_arm = {"value": r64["value"], "ms_per_step": r64["ms"] / a.steps,
-                    "mixed_speedup": value / r64["value"]}
+                    "mixed_speedup": value / r64["value"],
+                    "bn_zero_face_share": {"x": r64["bn_zero_share"][0],
+                                           "y": r64["bn_zero_share"][1]}}
         del r64
         torch.cuda.empty_cache()
         fp64_arm.update(_l1_mixed_vs_fp64(a, dev, a.steps))
@@ -463,6 +766,15 @@ def run_ours(a):
                "adjoint_over_forward": statistics.median(ratios),
                "J": mid["J"], "dJ_domega": mid["grad_omega"]}
 
+    extra = {}
+    if not a.no_extra:
+        del st, stepper
+        torch.cuda.empty_cache()
+        extra["later_state"] = _later_state_block(a, rp, dev)
+        extra["fp32"] = _fp32_block(a, rp, dev)
+        extra["vortex"] = _vortex_block(a, rp, dev)
+        extra["tubes"] = _tubes_block(a, rp, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -486,6 +798,7 @@ def run_ours(a):
                        "l2": "inputs exceed L2 (state >1 GB at 2048^2), no flush",
                        "bn_zero_face_share": {"x": bn0[0], "y": bn0[1]}},
             "fp64": fp64_arm,
+            **extra,
             "adjoint": adj,
             "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps,
@@ -496,7 +809,8 @@ def run_ours(a):
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
                                            "of the mixed sweep at 1536^2, scaled by faces",
                          "bytes_per_face": bytes_per_face,
-                         "avg_launch_ms": sweep_avg_s * 1e3, "share_of_step": sweep_share},
+                         "avg_launch_ms": sweep_avg_s * 1e3, "share_of_step": sweep_share,
+                         "fp64_pipe": fp64_pipe},
             "cpu_baseline": cpu,
             "clocks": clk,
         }

@@ -282,9 +282,11 @@ def rotor_forward(run: CheckpointedRun, grid, eos, rho0_phys, omega, dts, weight
     return float(magnetic_objective(grid, weight, out.Bxf, out.Byf, out.cons["Bz"]))
 
 
-def rotor_gradients(case: RotorCase, device="cuda"):
+def rotor_gradients(case: RotorCase, device="cuda", dts=None):
     """Forward + adjoint of the rotor study; returns J, dJ/d rho0 (physical
-    cells), dJ/d omega, the dt sequence and timings (CUDA events)."""
+    cells), dJ/d omega, the dt sequence and timings (CUDA events).  dts, when
+    given, is the frozen time-step sequence (its length overrides
+    case.steps); otherwise it is the CFL sequence of the unperturbed run."""
     from .physics.eos import hybrid_eos
     from .physics.grid import Grid2D
 
@@ -297,12 +299,15 @@ def rotor_gradients(case: RotorCase, device="cuda"):
     s0 = State2D(cons=_cons_from(prims, grid), Bxf=Bxf, Byf=Byf, prims={})
     run.stepper.sync(s0)
     # the dt sequence of the unperturbed run (frozen for the gradient)
-    s = s0.clone()
-    dts = []
-    for _ in range(case.steps):
-        dt = float(run.stepper.compute_dt(s, case.cfl).item())
-        dts.append(dt)
-        run.stepper.step(s, dt, "rk3")
+    if dts is None:
+        s = s0.clone()
+        dts = []
+        for _ in range(case.steps):
+            dt = float(run.stepper.compute_dt(s, case.cfl).item())
+            dts.append(dt)
+            run.stepper.step(s, dt, "rk3")
+    dts = [float(d) for d in dts]
+    case = RotorCase(case.n, len(dts), case.checkpoint_every, case.omega, case.cfl)
     def objective_adjoint(out):
         """J of the final state and its gradient as the adjoint's seed."""
         Bxf_o = out.Bxf.clone().requires_grad_(True)
@@ -341,3 +346,141 @@ def rotor_gradients(case: RotorCase, device="cuda"):
             "dts": dts, "run": run, "grid": grid, "eos": eos, "weight": weight,
             "forward_ms": e0.elapsed_time(e1), "adjoint_ms": e1.elapsed_time(e2),
             "rho0": prims["rho"][ph].clone()}
+
+
+# ── the discrete decisions a step freezes, and the finite-difference study ──
+
+def _tape_views(run: CheckpointedRun, k: int) -> dict:
+    """Views into tape k (the layout hlld_adjoint_record_step writes: two
+    stage-input states, then per stage the mass fluxes, p*, HLLE-fallback
+    flags and C2P roots of the sweeps, then three step diagnostics; every
+    array starts on a 256-byte boundary)."""
+    g = run.grid
+    nxt, nyt = g.nx + 2 * g.ng, g.ny + 2 * g.ng
+    nfx, nfy, nc = (nxt + 1) * nyt, nxt * (nyt + 1), nxt * nyt
+    raw = run._tapes[k]
+    off = run._tape(k) - raw.data_ptr()
+    views = {}
+
+    def take(name, count, dtype, size):
+        nonlocal off
+        views[name] = raw[off:off + count * size].view(dtype)
+        off += (count * size + 255) // 256 * 256
+
+    for x in range(2):
+        for i in range(6):
+            take(("X", x, "U", i), nc, torch.float64, 8)
+        take(("X", x, "Bxf"), nfx, torch.float64, 8)
+        take(("X", x, "Byf"), nfy, torch.float64, 8)
+        for i in range(9):
+            take(("X", x, "P", i), nc, torch.float64, 8)
+    for st in range(3):
+        take(("FxD", st), nfx, torch.float64, 8)
+        take(("FyD", st), nfy, torch.float64, 8)
+        take(("psx", st), nfx, torch.float64, 8)
+        take(("psy", st), nfy, torch.float64, 8)
+        take(("fx", st), nfx, torch.uint8, 1)
+        take(("fy", st), nfy, torch.uint8, 1)
+        take(("mu", st), nc, torch.float64, 8)
+    views["diag"] = raw[off:off + 3 * ctypes.sizeof(_lib.StepDiag)]
+    return views
+
+
+def _mc_branches(P: dict, grid) -> torch.Tensor:
+    """The MC limiter's branch (0: a b <= 0, no slope; 1, 2, 3: 2|a|, 2|b| or
+    |a + b| / 2 is the smallest) of every interior cell for the seven
+    reconstructed variables (rho, p, W v, transverse and normal B) along
+    both axes (reconstruction.py:69-77, 225-236)."""
+    v2 = P["vx"] ** 2 + P["vy"] ** 2 + P["vz"] ** 2
+    W = 1.0 / torch.sqrt(torch.clamp(1.0 - v2, min=1e-14))
+    fields = [P["rho"], P["p"], W * P["vx"], W * P["vy"], W * P["vz"], P["Bx"], P["By"], P["Bz"]]
+    codes = []
+    for axis in (0, 1):
+        for f in fields:
+            a = torch.diff(f, dim=axis)
+            lo = a.narrow(axis, 0, a.shape[axis] - 1)
+            hi = a.narrow(axis, 1, a.shape[axis] - 1)
+            c = 0.5 * (lo + hi)
+            m = torch.stack([2 * lo.abs(), 2 * hi.abs(), c.abs()]).argmin(dim=0) + 1
+            codes.append(torch.where(lo * hi > 0, m, torch.zeros_like(m)).to(torch.int8).flatten())
+    return torch.cat(codes)
+
+
+def step_decisions(run: CheckpointedRun, s: State2D, dt: float) -> dict:
+    """Advance the synced FP64 state s by one step (recording tape 0) and
+    return the discrete decisions of its three stages that the adjoint
+    freezes: the HLLE fallback of every x and y face, the CT upwind sign of
+    every face mass flux (ct.py:96-116, with its sweep-global deadband) and
+    the MC limiter branch of every cell, variable and axis."""
+    g = run.grid
+    nxt, nyt = g.nx + 2 * g.ng, g.ny + 2 * g.ng
+    inputs = [{k: s.prims[k].clone() for k in PRIM_KEYS}]
+    run.record_step(s, dt, 0)
+    v = _tape_views(run, 0)
+    for x in range(2):
+        inputs.append({k: v[("X", x, "P", i)].view(nxt, nyt) for i, k in enumerate(PRIM_KEYS)})
+    dsz = ctypes.sizeof(_lib.StepDiag)
+    out = {"fallback": [], "upwind": [], "limiter": []}
+    for st in range(3):
+        d = _lib.StepDiag.from_buffer_copy(bytes(v["diag"][st * dsz:(st + 1) * dsz].cpu().numpy()))
+        for axis, key in ((0, "FxD"), (1, "FyD")):
+            F = v[(key, st)]
+            scale = ctypes.c_double.from_buffer(ctypes.c_ulonglong(d.sweep[axis].fd_max_bits)).value
+            sgn = torch.where(F.abs() > 1e-9 * scale, torch.sign(F), torch.zeros_like(F))
+            out["upwind"].append(sgn.to(torch.int8))
+        out["fallback"] += [v[("fx", st)].clone(), v[("fy", st)].clone()]
+        out["limiter"].append(_mc_branches(inputs[st], g))
+    return {k: torch.cat(t) for k, t in out.items()}
+
+
+def decision_flips(run: CheckpointedRun, s_plus: State2D, s_minus: State2D, dts) -> dict:
+    """Count the frozen decisions that differ between two runs of the same dt
+    sequence (advanced in place): HLLE fallbacks, CT upwind signs and MC
+    limiter branches, summed over all steps and stages."""
+    flips = {"fallback": 0, "upwind": 0, "limiter": 0}
+    for dt in dts:
+        a = step_decisions(run, s_plus, dt)
+        b = step_decisions(run, s_minus, dt)
+        for k in flips:
+            flips[k] += int((a[k] != b[k]).sum())
+    return flips
+
+
+def rotor_fd_study(case: RotorCase, directions, h=1e-6, device="cuda"):
+    """Central differences of the rotor study's J along the given density
+    directions (and along omega) against the adjoint's directional
+    derivatives, with the decision flips between the +h and -h runs.
+    directions: callables (X, Y) -> field on the physical cells, X, Y the
+    cell-centre offsets from the rotor's centre.  Returns one record per
+    direction (omega first)."""
+    r = rotor_gradients(case, device=device)
+    run, grid, eos, w, dts = r["run"], r["grid"], r["eos"], r["weight"], r["dts"]
+    rho0 = r["rho0"]
+    X = grid.X[grid.phys] - 0.5
+    Y = grid.Y[grid.phys] - 0.5
+    records = []
+
+    def state(rho_phys, omega):
+        prims, Bxf, Byf = rotor_initial(grid, eos, rho_phys, omega)
+        s = State2D(cons=_cons_from(prims, grid), Bxf=Bxf, Byf=Byf, prims={})
+        run.stepper.sync(s)
+        return s
+
+    cases = [("omega", None, r["grad_omega"])]
+    for i, f in enumerate(directions):
+        d = f(X, Y)
+        cases.append((f"rho0[{i}]", d, float((r["grad_rho0"] * d).sum())))
+    for name, d, adj in cases:
+        if d is None:
+            sp, sm = state(rho0, case.omega + h), state(rho0, case.omega - h)
+        else:
+            sp, sm = state(rho0 + h * d, case.omega), state(rho0 - h * d, case.omega)
+        flips = decision_flips(run, sp.clone(), sm.clone(), dts)
+        for dt in dts:
+            run.stepper.step(sp, dt, "rk3")
+            run.stepper.step(sm, dt, "rk3")
+        J = lambda s: float(magnetic_objective(grid, w, s.Bxf, s.Byf, s.cons["Bz"]))
+        fd = (J(sp) - J(sm)) / (2 * h)
+        records.append({"direction": name, "fd": fd, "adjoint": adj, "flips": flips,
+                        "rel_err": abs(fd - adj) / max(abs(fd), 1e-300)})
+    return {"J": r["J"], "records": records, "n": case.n, "steps": len(dts), "h": h}

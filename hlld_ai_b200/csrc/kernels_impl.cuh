@@ -353,89 +353,106 @@ struct SweepParams {
     uint8_t *fail_out;
 };
 
-// One face of a directional sweep.  AXIS 0: faces (nxt+1, nyt), face f is
-// the lower-x face of cell (f, j).  AXIS 1: faces (nxt, nyt+1).
+// A directional sweep, one face per thread, on tiles of faces staged in
+// shared memory.  AXIS 0: faces (nxt+1, nyt), face f is the lower-x face of
+// cell (f, j); AXIS 1: faces (nxt, nyt+1).
+//
+// A CTA of 128 threads owns a tile of 4 x 32 faces: 4 rows along x by 32
+// along y, so a warp's 32 faces are consecutive in y and its loads and
+// stores are coalesced.  First the CTA fills the tile's stencil -- for the x
+// sweep (4 + 2S + 1) x 32 cells, for the y sweep 4 x (32 + 2S + 1) -- with
+// the seven reconstructed variables of every cell (rho, p, W vx, W vy, W vz,
+// the cell-centred transverse B, Bz; reconstruction.py:269 with vel_var Wv,
+// ct.py:44-54), each computed once instead of once per face that reads it;
+// then every thread reads its face's window from shared memory.  The
+// arithmetic per cell and per face is the per-face gather's, so the results
+// are the same bit for bit.
+constexpr int kTileAlong = 4;   // face rows along x per tile
+constexpr int kTileLanes = 32;  // face columns along y per tile
+
+template <int AXIS, int S> struct SweepTile {
+    static constexpr int ROWS = AXIS == 0 ? kTileAlong + 2 * S + 1 : kTileAlong;
+    static constexpr int COLS = AXIS == 0 ? kTileLanes : kTileLanes + 2 * S + 1;
+};
+
 template <int AXIS, int LIM, int SOLVER, bool EMF_HLL>
 __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(const SweepParams p) {
     using T = R;
     constexpr int S = Stencil<LIM>::S;
     constexpr int NW = 2 * S + 2;
+    constexpr int TR = SweepTile<AXIS, S>::ROWS, TC = SweepTile<AXIS, S>::COLS;
+    __shared__ T tile[7][TR][TC];
     const Grid &g = p.g;
     const int cols = AXIS == 0 ? g.nyt : g.nyt + 1;
     const int rows = AXIS == 0 ? g.nxt + 1 : g.nxt;
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = AXIS == 0 ? g.nxt : g.nyt;  // cells along the sweep axis
+    const int tiles_y = (cols + kTileLanes - 1) / kTileLanes;
+    const int row0 = (int)(blockIdx.x / tiles_y) * kTileAlong;  // first face row (x)
+    const int col0 = (int)(blockIdx.x % tiles_y) * kTileLanes;  // first face column (y)
+    // the window of the tile's first face starts at cell c0 along the sweep
+    // axis; cells outside [0, n) are clamped (the edge rules never read them)
+    const int c0 = (AXIS == 0 ? row0 : col0) - 1 - S;
+    // transverse in-plane B at cell (i, j), averaged from its faces (ct.py:44-54)
+    auto bt_at = [&](int i, int j) -> T {
+        return AXIS == 0
+                   ? T(RS(0.5) * (p.Byf[(int64_t)i * (g.nyt + 1) + j] + p.Byf[(int64_t)i * (g.nyt + 1) + j + 1]))
+                   : T(RS(0.5) * (p.Bxf[(int64_t)i * g.nyt + j] + p.Bxf[(int64_t)(i + 1) * g.nyt + j]));
+    };
+    for (int q = threadIdx.x; q < TR * TC; q += blockDim.x) {
+        const int r = q / TC, cc = q - r * TC;
+        int i = AXIS == 0 ? c0 + r : row0 + r;
+        int j = AXIS == 0 ? col0 + cc : c0 + cc;
+        if (AXIS == 0) {
+            i = i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
+            if (j > g.nyt - 1) continue;
+        } else {
+            j = j < 0 ? 0 : (j > n - 1 ? n - 1 : j);
+            if (i > g.nxt - 1) continue;
+        }
+        const int64_t ci = (int64_t)i * g.nyt + j;
+        T vx = p.vx[ci], vy = p.vy[ci], vz = p.vz[ci];
+        T v2 = vx * vx + vy * vy + vz * vz;
+        T W = T(1) / sqrt(clamp_lo(T(1) - v2, T(1e-14)));
+        tile[0][r][cc] = p.rho[ci];
+        tile[1][r][cc] = p.p[ci];
+        tile[2][r][cc] = W * vx;
+        tile[3][r][cc] = W * vy;
+        tile[4][r][cc] = W * vz;
+        tile[5][r][cc] = bt_at(i, j);
+        tile[6][r][cc] = p.bz[ci];
+    }
+    __syncthreads();
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int row = row0 + w, col = col0 + l;
     Counts cnt = {};
-    const bool live = e < (int64_t)rows * cols;
+    const bool live = row < rows && col < cols;
     if (live) {
-        const int row = (int)(e / cols), col = (int)(e - (int64_t)row * cols);
         const int f = AXIS == 0 ? row : col;   // face index along the sweep axis
         const int tr = AXIS == 0 ? col : row;  // transverse index
-        const int n = AXIS == 0 ? g.nxt : g.nyt;
-        const int64_t cstride = AXIS == 0 ? g.nyt : 1;
-        const int64_t cbase = AXIS == 0 ? (int64_t)tr : (int64_t)tr * g.nyt;
-        // transverse in-plane B at cell c, averaged from its faces (ct.py:44-54)
-        auto bt_at = [&](int c) -> T {
-            return AXIS == 0
-                       ? T(RS(0.5) * (p.Byf[(int64_t)c * (g.nyt + 1) + tr] + p.Byf[(int64_t)c * (g.nyt + 1) + tr + 1]))
-                       : T(RS(0.5) * (p.Bxf[(int64_t)tr * g.nyt + c] + p.Bxf[(int64_t)(tr + 1) * g.nyt + c]));
-        };
-        // work variables (reconstruction.py:269): rho, p, W vx, W vy, W vz,
-        // transverse in-plane B, Bz
+        // tile entry of window cell k (cell f - 1 - S + k) of this face
+        auto at = [&](int v, int k) -> T { return AXIS == 0 ? tile[v][w + k][l] : tile[v][w][l + k]; };
         T L[7], Rt[7];
         if (f == 0 || f == n) {
-            // outermost faces: the edge cell has zero slope in every scheme
-            const int c = f == 0 ? 0 : n - 1;
-            const int64_t ci = cbase + c * cstride;
-            T vx = p.vx[ci], vy = p.vy[ci], vz = p.vz[ci];
-            T v2 = vx * vx + vy * vy + vz * vz;
-            T W = T(1) / sqrt(clamp_lo(T(1) - v2, T(1e-14)));
-            T q[7] = {p.rho[ci], p.p[ci], W * vx, W * vy, W * vz, bt_at(c), p.bz[ci]};
+            // outermost faces: the edge cell (0 or n - 1) has zero slope in
+            // every scheme
+            const int k = f == 0 ? S + 1 : S;
 #pragma unroll
-            for (int k = 0; k < 7; ++k) {
-                L[k] = q[k] + T(0.5) * T(0);
-                Rt[k] = q[k] - T(0.5) * T(0);
+            for (int v = 0; v < 7; ++v) {
+                const T q = at(v, k);
+                L[v] = q + T(0.5) * T(0);
+                Rt[v] = q - T(0.5) * T(0);
             }
         } else {
-            // window of cells f-1-S .. f+S (clamped; clamped entries are never
-            // read by the edge rules)
-            int cw[NW];
-#pragma unroll
-            for (int k = 0; k < NW; ++k) {
-                int c = f - 1 - S + k;
-                cw[k] = c < 0 ? 0 : (c > n - 1 ? n - 1 : c);
-            }
-            T Wf[NW];
-#pragma unroll
-            for (int k = 0; k < NW; ++k) {
-                const int64_t ci = cbase + cw[k] * cstride;
-                T vx = p.vx[ci], vy = p.vy[ci], vz = p.vz[ci];
-                T v2 = vx * vx + vy * vy + vz * vz;
-                Wf[k] = T(1) / sqrt(clamp_lo(T(1) - v2, T(1e-14)));
-            }
             T pcmL[7], pcmR[7];
 #pragma unroll
             for (int v = 0; v < 7; ++v) {
-                T w[NW];
+                T wv[NW];
 #pragma unroll
-                for (int k = 0; k < NW; ++k) {
-                    const int c = cw[k];
-                    const int64_t ci = cbase + c * cstride;
-                    T x;
-                    switch (v) {
-                    case 0: x = p.rho[ci]; break;
-                    case 1: x = p.p[ci]; break;
-                    case 2: x = Wf[k] * p.vx[ci]; break;
-                    case 3: x = Wf[k] * p.vy[ci]; break;
-                    case 4: x = Wf[k] * p.vz[ci]; break;
-                    case 5: x = bt_at(c); break;
-                    default: x = p.bz[ci]; break;
-                    }
-                    w[k] = x;
-                }
-                L[v] = cell_edge<LIM, true, S>(w, f - 1, n);
-                Rt[v] = cell_edge<LIM, false, S + 1>(w, f, n);
-                pcmL[v] = w[S];
-                pcmR[v] = w[S + 1];
+                for (int k = 0; k < NW; ++k) wv[k] = at(v, k);
+                L[v] = cell_edge<LIM, true, S>(wv, f - 1, n);
+                Rt[v] = cell_edge<LIM, false, S + 1>(wv, f, n);
+                pcmL[v] = wv[S];
+                pcmR[v] = wv[S + 1];
             }
             if (LIM != HLLD_LIM_PCM) {
                 // positivity fallback to PCM (reconstruction.py:315-326)
@@ -486,7 +503,7 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
             constexpr int KB = AXIS == 0 ? C_BY : C_BX;
             o.F[KB] = hf(ph.L.f[KB], ph.R.f[KB], ph.L.u[KB], ph.R.u[KB], ph.cmin, ph.cmax);
         }
-        const int64_t fi = e;
+        const int64_t fi = (int64_t)row * cols + col;
         p.F[F_D][fi] = o.F[C_D];
         p.F[F_SX][fi] = o.F[C_SX];
         p.F[F_SY][fi] = o.F[C_SY];
@@ -1272,13 +1289,17 @@ static Grid make_grid(const hlld_grid2d_t *g) {
 
 template <int AXIS, int LIM, bool EMF_HLL>
 static void launch_sweep_emf(int solver, const SweepParams &sp, cudaStream_t st) {
-    const int64_t nf = AXIS == 0 ? (int64_t)(sp.g.nxt + 1) * sp.g.nyt : (int64_t)sp.g.nxt * (sp.g.nyt + 1);
+    static_assert(kThreads == kTileAlong * kTileLanes, "one face per thread of a tile");
+    const int rows = AXIS == 0 ? sp.g.nxt + 1 : sp.g.nxt;
+    const int cols = AXIS == 0 ? sp.g.nyt : sp.g.nyt + 1;
+    const unsigned nb = (unsigned)((int64_t)((rows + kTileAlong - 1) / kTileAlong) *
+                                   ((cols + kTileLanes - 1) / kTileLanes));
     if (solver == HLLD_SOLVER_HLLD)
-        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLD, EMF_HLL><<<grid1d(nf), kThreads, 0, st>>>(sp);
+        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLD, EMF_HLL><<<nb, kThreads, 0, st>>>(sp);
     else if (solver == HLLD_SOLVER_HLLC)
-        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLC, EMF_HLL><<<grid1d(nf), kThreads, 0, st>>>(sp);
+        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLC, EMF_HLL><<<nb, kThreads, 0, st>>>(sp);
     else
-        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLE, EMF_HLL><<<grid1d(nf), kThreads, 0, st>>>(sp);
+        sweep_kernel<AXIS, LIM, HLLD_SOLVER_HLLE, EMF_HLL><<<nb, kThreads, 0, st>>>(sp);
 }
 
 // the HLL face EMF is a separate instantiation, so that the default sweep

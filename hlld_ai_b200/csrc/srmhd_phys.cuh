@@ -105,14 +105,20 @@ template <typename T> __device__ __forceinline__ T sdiv(T num, T den) {
 // y <- y + y (1 - d y) squares the relative error: the hardware's
 // approximate reciprocal as the seed and three steps, which leave an error of
 // a few ulp.  Used by the mixed form's FP64 p* solve and cell C2P
-// (HLLD_NR_RCP), whose tolerances are far above it.  Outside 2^-1000 <= |d|
-// < 2^1000 (zero, subnormals, where the seed's flush-to-zero would give 0 or
-// inf, huge values whose reciprocal is subnormal, inf and NaN) it divides, so
-// that every input gets the quotient 1.0 / d would give.
+// (HLLD_NR_RCP), whose tolerances are far above it.
+//
+// Domain: finite d with 2^-1000 <= |d| < 2^1000.  The seed flushes to zero
+// outside it, so d = +-inf gives NaN (1 / d would give 0), |d| >= 2^1022
+// gives 0 (1 / d a subnormal) and |d| < 2^-1022 gives inf; a NaN gives NaN
+// like the division.  The callers stay inside: SharedDen clamps |d| to at
+// least 1e-300 (the reference's _sdiv rule), the p* residual's denominators
+// are finite for finite face states, and the Kastaun master function takes
+// reciprocals of 1 / W in [1e-5, 1], of 1 + W, of rho (1 + eps) in
+// [1e-12, 1e20] and of 1 + mu |B~|^2 >= 1, which leaves the domain only for
+// |B~|^2 = B^2 / D above 1e300, not a finite physical state.  (A check of the
+// domain at every call made the mixed sweep 13 % slower, so there is none.)
 __device__ __forceinline__ double nr_rcp(double d) {
 #if defined(__CUDA_ARCH__)
-    const double a = fabs(d);
-    if (!(a < 0x1p1000 && a >= 0x1p-1000)) return 1.0 / d;
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
 #pragma unroll

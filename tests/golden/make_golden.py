@@ -25,6 +25,11 @@ inputs, the outputs the oracle is pinned against (tests/test_oracle_golden.py):
                HLL face EMF, ct.py:63-88) of the rotor and the Orszag-Tang
                vortex, HLLD and HLLE (``python make_golden.py REF emf_hll``
                writes only this file)
+  rotor_gradient.npz  the gradient of J = sum w |B|^2 / 2 through
+               rk_step_ct on the tapered rotor, by central differences of
+               the reference and by shimmed torch autograd (``python
+               make_golden.py REF gradient N STEPS``, only this file; see
+               make_gradient)
 
 The reference is not needed to run the tests; only this script reads it.
 """
@@ -404,14 +409,147 @@ def make_emf_hll(ref_root: str) -> None:
     print("emf_hll.npz written to", HERE)
 
 
+def make_gradient(ref_root: str, n: int = 128, steps: int = 4) -> None:
+    """rotor_gradient.npz: the reference's gradient of the config-5 objective
+    on the tapered rotor at n^2 after `steps` FP64 HLLD + PLM-MC + SSP-RK3 +
+    CT steps of rk_step_ct (driver2d.py:221-249, periodic), the dt sequence
+    frozen: J = sum over cells of w |B_c|^2 / 2 (Gaussian w at (0.6, 0.5),
+    sigma 0.1), with respect to omega and to the initial density field.
+
+    Two estimates are recorded:
+      * central differences of the reference itself: d J / d omega at
+        h = 1e-5 and 1e-6, and d J / d rho0 along the eight seeded directions
+        of gradient_directions at h = 1e-5 and 2e-5 (a pair that agrees
+        marks a direction whose perturbed runs take the same discrete
+        decisions, limiter branches, HLLD fallbacks, CT upwind signs);
+      * torch autograd through the reference.  As shipped it cannot be
+        differentiated: its C2P, boundary fills and sync write in place into
+        tensors autograd has saved, and every torch.where whose unselected
+        branch divides by a tiny number or takes the square root of 0 sends
+        0 * inf = NaN into the backward pass.  Here wrappers hand the
+        in-place writes fresh copies (KastaunC2P.invert / invert_bisection
+        results, the arrays apply_bc_cc fills, the state sync_state fills),
+        which changes no forward value, and a hook on every backward node
+        sets non-finite input gradients to zero.  The result is recorded as
+        it comes out; it does not agree with the central differences."""
+    sys.dont_write_bytecode = True
+    os.environ.pop("RMHD_PSTAR_METHOD", None)
+    sys.path.insert(0, ref_root)
+    import torch
+    import src.physics.c2p as C
+    import src.physics.driver2d as D
+    import src.physics.grid as GR
+    from src.physics.eos import hybrid_eos
+    from src.physics.initial_data2d import b_from_potential
+    from src.physics.state import EVOLVED_KEYS, State2D
+
+    torch.set_num_threads(os.cpu_count() or 1)
+    G = 5.0 / 3.0
+    eos = hybrid_eos(K=0.0, gamma=G, gamma_th=G)
+    g = GR.Grid2D(0.0, 1.0, n, 0.0, 1.0, n, ng=2)
+    X, Y = g.X - 0.5, g.Y - 0.5
+    f = ((0.115 - torch.sqrt(X * X + Y * Y)) / 0.015).clamp(0.0, 1.0)
+    w = torch.exp(-((g.X - 0.6) ** 2 + (g.Y - 0.5) ** 2) / (2 * 0.1 ** 2))
+    ph = g.phys
+    _, YF = torch.meshgrid(g.xf, g.yf, indexing="ij")
+
+    def run(rho, omega, dts=None):
+        zero = torch.zeros_like(f)
+        prims = {"rho": rho, "p": torch.ones_like(f), "vx": -omega * Y * f, "vy": omega * X * f,
+                 "vz": zero, "Bx": torch.ones_like(f), "By": zero.clone(), "Bz": zero.clone()}
+        prims["eps"] = eos.eps__press_rho(prims["p"], prims["rho"])
+        Bxf, Byf = b_from_potential(YF.clone(), g.dx, g.dy)
+        c = D.prims_to_cons_2d(prims, g)
+        st = State2D(cons={k: c[k] for k in EVOLVED_KEYS}, Bxf=Bxf, Byf=Byf, prims=prims)
+        st = D.sync_state(st, g, eos, "periodic", "periodic")
+        out = []
+        for k in range(steps):
+            if dts is None:
+                with torch.no_grad():
+                    dt = D.compute_dt_2d({q: v.detach() for q, v in st.prims.items()}, g, eos, 0.4)
+            else:
+                dt = dts[k]
+            out.append(dt)
+            st, _ = D.rk_step_ct(st, g, eos, dt, scheme="rk3", bc_x="periodic", bc_y="periodic")
+        B2 = st.prims["Bx"] ** 2 + st.prims["By"] ** 2 + st.prims["Bz"] ** 2
+        return (w[ph] * B2[ph]).sum() / 2, out
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    from helpers import gradient_directions
+
+    rho_base = 1.0 + 9.0 * f
+    with torch.no_grad():
+        J0, dts = run(rho_base, 9.95)
+        fd_omega = [float((run(rho_base, 9.95 + h, dts)[0] - run(rho_base, 9.95 - h, dts)[0])
+                          / (2 * h)) for h in (1e-5, 1e-6)]
+        fd_dir = np.zeros((8, 2))
+        full = torch.zeros_like(f)
+        for k in range(8):
+            dirn = full.clone()
+            dirn[ph] = gradient_directions(X[ph], Y[ph], k)
+            for j, h in enumerate((1e-5, 2e-5)):
+                fd_dir[k, j] = float((run(rho_base + h * dirn, 9.95, dts)[0]
+                                      - run(rho_base - h * dirn, 9.95, dts)[0]) / (2 * h))
+            print("direction", k, fd_dir[k], flush=True)
+
+    # torch autograd through the reference, shimmed as described above
+    inv, bis = C.KastaunC2P.invert, C.KastaunC2P.invert_bisection
+    C.KastaunC2P.invert = lambda self, *a, **k: {q: v.clone() for q, v in inv(self, *a, **k).items()}
+    C.KastaunC2P.invert_bisection = lambda self, *a, **k: {q: v.clone()
+                                                           for q, v in bis(self, *a, **k).items()}
+    bc_cc = GR.Grid2D.apply_bc_cc
+
+    def fresh_bc_cc(self, U, *a, **k):
+        for q in list(U):
+            U[q] = U[q].clone()
+        return bc_cc(self, U, *a, **k)
+
+    GR.Grid2D.apply_bc_cc = fresh_bc_cc
+    sync = D.sync_state
+
+    def fresh_sync(state, *a, **k):
+        state.Bxf, state.Byf = state.Bxf.clone(), state.Byf.clone()
+        state.cons = {q: v.clone() for q, v in state.cons.items()}
+        return sync(state, *a, **k)
+
+    D.sync_state = fresh_sync
+    rho0 = rho_base.clone().requires_grad_(True)
+    omega = torch.tensor(9.95, dtype=torch.float64, requires_grad=True)
+    J, _ = run(rho0, omega, dts)
+
+    def finite(grad_inputs, grad_outputs):
+        return tuple(None if x is None else torch.nan_to_num(x, nan=0.0, posinf=0.0, neginf=0.0)
+                     for x in grad_inputs)
+
+    seen, todo = set(), [J.grad_fn]
+    while todo:
+        node = todo.pop()
+        if node is None or node in seen:
+            continue
+        seen.add(node)
+        node.register_hook(finite)
+        todo.extend(nx for nx, _ in node.next_functions)
+    J.backward()
+    np.savez_compressed(os.path.join(HERE, "rotor_gradient.npz"), n=n, steps=steps,
+                        dts=np.array(dts), J=float(J0), fd_omega=np.array(fd_omega),
+                        fd_h_omega=np.array([1e-5, 1e-6]), fd_dir=fd_dir,
+                        fd_h_dir=np.array([1e-5, 2e-5]),
+                        autograd_omega=float(omega.grad), autograd_rho0=rho0.grad[ph].numpy())
+    print("rotor_gradient.npz written to", HERE, "J", float(J0), "FD dJ/domega", fd_omega,
+          "autograd", float(omega.grad))
+
+
 if __name__ == "__main__":
     if len(sys.argv) < 2:
-        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_CHECKOUT [hllc|emf_hll]")
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_CHECKOUT "
+                 "[hllc | emf_hll | gradient N STEPS]")
     root = sys.argv[1]
     if len(sys.argv) > 2 and sys.argv[2] == "hllc":
         make_hllc(root)
     elif len(sys.argv) > 2 and sys.argv[2] == "emf_hll":
         make_emf_hll(root)
+    elif len(sys.argv) > 2 and sys.argv[2] == "gradient":
+        make_gradient(root, *(int(x) for x in sys.argv[3:5]))
     else:
         main(root)
         make_hllc(root)

@@ -91,3 +91,30 @@ def bitwise_equal(a, b) -> bool:
     a = np.asarray(a)
     b = np.asarray(b)
     return bool(np.all((a == b) | (np.isnan(a) & np.isnan(b))))
+
+
+def gradient_directions(X, Y, k):
+    """Seeded density perturbation directions of the gradient fixture, as
+    functions of the cell-centre offsets (X, Y) from the rotor's centre:
+    k = 0..3 (and even k >= 8) a sum of three random-phase sinusoids over
+    the whole domain, k = 4..7 (and odd k >= 8) a random-phase ring mode
+    cos(m theta + phi) on the rotor's
+    taper (0.1 < r < 0.115, where the density varies and the limiter is away
+    from its kink).  tests/golden/make_golden.py evaluates them on the CPU for
+    the reference's central differences, the GPU tests on the device."""
+    import math
+
+    rng = np.random.default_rng(1000 + k)
+    if k < 4 or (k >= 8 and k % 2 == 0):
+        d = 0.0
+        for _ in range(3):
+            kx, ky = rng.integers(1, 4, 2)
+            ph = rng.uniform(0, 2 * math.pi)
+            d = d + (2 * math.pi * (kx * X + ky * Y) + ph).cos()
+        return d / 3.0
+    m = int(rng.integers(1, 6))
+    ph = rng.uniform(0, 2 * math.pi)
+    r = (X * X + Y * Y).sqrt()
+    theta = Y.atan2(X)
+    ring = ((r - 0.1) * (0.115 - r)).clamp(min=0.0) / (0.0075 ** 2)
+    return (m * theta + ph).cos() * ring

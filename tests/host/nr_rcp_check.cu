@@ -4,13 +4,10 @@
 //
 // Inputs: n doubles of both signs with exponents spread over [1e-300, 1e300]
 // and random mantissas (a fixed-seed LCG on the host), the two ends of the
-// Newton range (2^-1000 and the double just below 2^1000, both signs), and
-// the inputs outside it (zeros, subnormals, the double just below 2^-1000,
-// +-2^1000, 2^1023, +-DBL_MAX, +-inf, NaN), whose results must have the bit
-// pattern of 1.0 / d.  Output: one line "max_ulp <k> n=<n> edge_mismatch=<m>";
-// exit status 1 if any input of the range gives a result more than `bound`
-// ulp (default 2) from 1.0 / d or not finite, or any input outside it gives
-// another bit pattern than 1.0 / d.
+// documented domain 2^-1000 <= |d| < 2^1000 (both signs), and a NaN, whose
+// result must be a NaN.  Output: one line "max_ulp <k> n=<n> nan_ok=<0|1>";
+// exit status 1 if any result of the domain is more than `bound` ulp
+// (default 2) from 1.0 / d or not finite, or the NaN does not give a NaN.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -32,17 +29,12 @@ int main(int argc, char **argv) {
     const long long bound = argc > 1 ? atoll(argv[1]) : 2;
     const double ends[] = {0x1p-1000, -0x1p-1000, nextafter(0x1p1000, 0.0),
                            -nextafter(0x1p1000, 0.0)};
-    const double edge[] = {0.0, -0.0, 4.9e-324, -4.9e-324, 2.2e-308, -2.2e-308,
-                           nextafter(0x1p-1000, 0.0), 0x1p1000, -0x1p1000, 0x1p1023,
-                           -0x1p1023, 1.7976931348623157e308, -1.7976931348623157e308,
-                           INFINITY, -INFINITY, NAN};
     const int nends = (int)(sizeof(ends) / sizeof(ends[0]));
-    const int ne = (int)(sizeof(edge) / sizeof(edge[0]));
-    const int nr = (1 << 20) + nends;  // inputs inside the Newton range
-    const int n = nr + ne;
+    const int nr = (1 << 20) + nends;  // inputs of the domain
+    const int n = nr + 1;              // and a NaN
     std::vector<double> h(n), a(n), b(n);
     uint64_t s = 88172645463325252ull;
-    for (int k = 0; k < ne; ++k) h[nr + k] = edge[k];
+    h[nr] = NAN;
     for (int k = 0; k < nends; ++k) h[nr - nends + k] = ends[k];
     for (int i = 0; i < nr - nends; ++i) {
         s = s * 6364136223846793005ull + 1442695040888963407ull;
@@ -64,14 +56,7 @@ int main(int argc, char **argv) {
     cudaFree(dr);
     long long worst = 0;
     bool bad = false;
-    int edge_mismatch = 0;
-    for (int i = nr; i < n; ++i) {
-        const bool same = (std::isnan(a[i]) && std::isnan(b[i])) || memcmp(&a[i], &b[i], 8) == 0;
-        if (!same) {
-            ++edge_mismatch;
-            printf("edge d=%a nr=%a div=%a\n", h[i], a[i], b[i]);
-        }
-    }
+    const bool nan_ok = std::isnan(a[nr]) && std::isnan(b[nr]);
     for (int i = 0; i < nr; ++i) {
         if (!std::isfinite(a[i])) { bad = true; continue; }
         int64_t ia, ib;
@@ -80,6 +65,6 @@ int main(int argc, char **argv) {
         const long long du = llabs((long long)(ia - ib));
         if (du > worst) worst = du;
     }
-    printf("max_ulp %lld n=%d edge_mismatch=%d\n", worst, nr, edge_mismatch);
-    return (bad || worst > bound || edge_mismatch) ? 1 : 0;
+    printf("max_ulp %lld n=%d nan_ok=%d\n", worst, nr, nan_ok ? 1 : 0);
+    return (bad || worst > bound || !nan_ok) ? 1 : 0;
 }
