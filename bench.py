@@ -75,9 +75,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint/forward cost of the 512^2 rotor gradient study")
-    ap.add_argument("--workload", default="rotor", choices=["rotor", "tubes", "adjoint"],
+    ap.add_argument("--workload", default="rotor",
+                    choices=["rotor", "tubes", "adjoint", "vortex", "rotor_run"],
                     help="rotor: the 2D rotor step (default); tubes: the batched-tube launch; "
-                         "adjoint: the rotor gradient study alone (adjoint/forward cost)")
+                         "adjoint: the rotor gradient study alone (adjoint/forward cost); "
+                         "vortex: the vortex block alone (--vortex-n, --vortex-tend); "
+                         "rotor_run: whole rotor runs to --tend in every precision")
+    ap.add_argument("--tend", type=float, default=0.4, help="rotor_run: end time")
     ap.add_argument("--adjoint-n", type=int, default=512)
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint interval")
@@ -1020,6 +1024,78 @@ def run_adjoint(a):
     return 0
 
 
+def run_vortex(a):
+    """The vortex block alone (config 3) as its own line."""
+    import torch
+
+    from hlld_ai_b200 import replicas
+
+    rp = replicas.from_env("cuda")
+    torch.cuda.set_device(rp.local)
+    replicas.init(rp)
+    res = _vortex_block(a, rp, rp.device)
+    replicas.finish(rp)
+    if rp.rank == 0:
+        print(json.dumps({"metric": "zone-updates/s", "value": res["mixed"]["value"],
+                          "unit": "zone-updates/s", "n_gpus": rp.world, "higher_is_better": True,
+                          "dtype": "f32+f64", "data": "synthetic",
+                          "config": {"workload": "relativistic vortex 2D, periodic [0,1]^2, "
+                                                 "gamma 4/3, HLLD + PLM(MC, Wv) + SSP-RK3 + CT",
+                                     "n": a.n},
+                          "vortex": res}), flush=True)
+    return 0
+
+
+def run_rotor_whole(a):
+    """Whole rotor runs from t = 0 to a.tend at a.n^2 in the mixed, FP32 and
+    FP64 forms, all with the FP64 run's CFL dt sequence: each form's mean
+    zone-updates/s over the run (CUDA events around every step, the dt
+    computation of the FP64 run excluded) and the density L1/Linf of the
+    mixed and FP32 runs against FP64 at a.tend."""
+    import torch
+
+    from hlld_ai_b200 import replicas
+
+    rp = replicas.from_env("cuda")
+    dev = rp.device
+    torch.cuda.set_device(rp.local)
+    replicas.init(rp)
+    runs = {p: _stepper(PROBLEM, a.n, p, dev) for p in ("fp64", "mixed", "fp32")}
+    stream = torch.cuda.current_stream(dev)
+    ms = {p: 0.0 for p in runs}
+    t, steps = 0.0, 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    while t < a.tend - 1e-14:
+        dt = min(float(runs["fp64"][2].compute_dt(runs["fp64"][1], a.cfl).item()), a.tend - t)
+        for p, (g, st, stp) in runs.items():
+            e0.record(stream)
+            stp.step(st, dt, "rk3")
+            e1.record(stream)
+            e1.synchronize()
+            ms[p] += e0.elapsed_time(e1)
+        t += dt
+        steps += 1
+    ph = runs["fp64"][0].phys
+    ref = runs["fp64"][1].prims["rho"][ph]
+    zones = a.n * a.n * rp.world
+    out = {"n": a.n, "t": t, "steps": steps}
+    for p in runs:
+        (m,) = replicas.max_over_ranks(rp, ms[p])
+        out[p] = {"ms_per_step": m / steps, "value": zones * steps / (m * 1e-3)}
+        if p != "fp64":
+            d = (runs[p][1].prims["rho"][ph].double() - ref).abs()
+            out[p].update(l1_rho=float(d.mean()), linf_rho=float(d.max()))
+    replicas.finish(rp)
+    if rp.rank == 0:
+        print(json.dumps({"metric": "zone-updates/s", "value": out["mixed"]["value"],
+                          "unit": "zone-updates/s", "n_gpus": rp.world, "higher_is_better": True,
+                          "dtype": "f32+f64", "data": "synthetic",
+                          "config": {"workload": WORKLOAD + f", whole run to t = {a.tend}",
+                                     "n": a.n},
+                          "rotor_run": out}), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -1028,6 +1104,10 @@ def main():
         return run_tubes(a)
     if a.workload == "adjoint":
         return run_adjoint(a)
+    if a.workload == "vortex":
+        return run_vortex(a)
+    if a.workload == "rotor_run":
+        return run_rotor_whole(a)
     return run_ours(a)
 
 

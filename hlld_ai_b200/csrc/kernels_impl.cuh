@@ -489,7 +489,8 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         }
         FaceOut<T> o;
         if (SOLVER == HLLD_SOLVER_HLLD)
-            hlld_face<AXIS, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)g.gamma, false, o);
+            hlld_face<AXIS, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)g.gamma, false, o, nullptr,
+                                                            p.pstar_out != nullptr);
         else if (SOLVER == HLLD_SOLVER_HLLC)
             hllc_face<AXIS, T>(PL, PR, (T)g.gamma, false, o);
         else
@@ -963,7 +964,7 @@ __device__ __forceinline__ void tube_face(const TubesParams &p, int64_t base, in
     }
     FaceOut<T> o;
     if (SOLVER == HLLD_SOLVER_HLLD)
-        hlld_face<0, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)p.gamma, false, o);
+        hlld_face<0, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)p.gamma, false, o, nullptr, false);
     else
         hlle_face<0, T>(PL, PR, (T)p.gamma, false, false, o);
 #pragma unroll
@@ -997,7 +998,7 @@ __device__ __forceinline__ void tube_face_driver1d(const TubesParams &p, int64_t
     }
     FaceOut<T> o;
     if (SOLVER == HLLD_SOLVER_HLLD)
-        hlld_face<0, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)p.gamma, false, o);
+        hlld_face<0, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)p.gamma, false, o, nullptr, false);
     else
         hlle_face<0, T>(PL, PR, (T)p.gamma, false, false, o);
 #pragma unroll

@@ -1071,11 +1071,14 @@ template <typename TP> __device__ __forceinline__ TP hlld_ift_root(const HlldR<T
 // IFT = true is the tangent form (T = TP = Dual): given[0] is the face's
 // solved p* and given[1] != 0 its fallback decision, both from the value
 // computation; the bracket and the secant are skipped.  SKIP_BN0: no p*
-// solve on faces without normal field (see below).
+// solve on faces without normal field (see below); with need_pstar false as
+// well, not even the HLL-state C2P whose total pressure would only feed the
+// p* output there (o.pstar is then 0).
 template <int IDIR, typename T, typename TC = T, typename TP = T, bool IFT = false,
           bool SKIP_BN0 = (sizeof(TC) == sizeof(float))>
 __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, bool want_u,
-                                          FaceOut<T> &o, const double *given = nullptr) {
+                                          FaceOut<T> &o, const double *given = nullptr,
+                                          bool need_pstar = true) {
     constexpr int i = IDIR, t1 = (IDIR + 1) % 3, t2 = (IDIR + 2) % 3;
     Phys<T> ph;
     srmhd_fluxes<IDIR>(PL, PR, gamma, ph);
@@ -1087,9 +1090,26 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         uH[k] = hu(ph.L.f[k], ph.R.f[k], ph.L.u[k], ph.R.u[k], cm, cx);
     }
 
+    constexpr int Sn = C_SX + i, Bn = C_BX + i;
+    if constexpr (!IFT && SKIP_BN0) {
+        // a face without normal field whose p* output nobody reads: the
+        // HLLE fallback's flux and state, nothing else (hlld.py:1512-1531)
+        if (!need_pstar && fabs(ph.L.u[Bn]) < T(1e-14) && fabs(ph.R.u[Bn]) < T(1e-14)) {
+#pragma unroll
+            for (int k = 0; k < NCONS; ++k) {
+                o.F[k] = fH[k];
+                if (want_u) o.U[k] = uH[k];
+            }
+            o.pstar = T(0);
+            o.err = -1;
+            o.iters = 0;
+            o.flags = RF_BN_ZERO | RF_FAILED;
+            return;
+        }
+    }
+
     // legacy bracket (hlld.py:1253-1263): total pressure of the HLL state
     TP p_hll = TP(0), p_lo = TP(0), p_hi = TP(0);
-    constexpr int Sn = C_SX + i, Bn = C_BX + i;
     if constexpr (!IFT) {
         TC Ch[NCONS], Ph[NPRIM];
 #pragma unroll
