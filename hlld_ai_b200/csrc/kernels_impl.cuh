@@ -489,8 +489,8 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         }
         FaceOut<T> o;
         if (SOLVER == HLLD_SOLVER_HLLD)
-            hlld_face<AXIS, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)g.gamma, false, o, nullptr,
-                                                            p.pstar_out != nullptr);
+            hlld_face<AXIS, T, RB, RS, false, kSkipBnZero, true>(PL, PR, (T)g.gamma, false, o,
+                                                                  nullptr, p.pstar_out != nullptr);
         else if (SOLVER == HLLD_SOLVER_HLLC)
             hllc_face<AXIS, T>(PL, PR, (T)g.gamma, false, o);
         else

@@ -1045,6 +1045,14 @@ template <typename T> __device__ __forceinline__ T hlld_residual(const HlldR<T> 
     if constexpr (sizeof(T) <= sizeof(double)) return hlld_residual_ool(c, p);
     else return hlld_residual_body(c, p);
 }
+// The residual at a p* solve's call sites: inlined for the 2D sweeps
+// (INLINE = true; measured on B200: the mixed x sweep 1.084 -> 1.000 ms,
+// the FP64 one 2.62 -> 2.39 ms), out of line for the tube kernel, whose
+// phases share the instruction cache.
+template <bool INLINE, typename T> __device__ __forceinline__ T hlld_residual_at(const HlldR<T> &c, T p) {
+    if constexpr (INLINE) return hlld_residual_body(c, p);
+    else return hlld_residual(c, p);
+}
 
 #define HLLD_R_FIELDS(X)                                                                        \
     X(RSiL) X(RSiR) X(RS1L) X(RS1R) X(RS2L) X(RS2R) X(RBiL) X(RBiR) X(RB1L) X(RB1R) X(RB2L)      \
@@ -1073,9 +1081,10 @@ template <typename TP> __device__ __forceinline__ TP hlld_ift_root(const HlldR<T
 // computation; the bracket and the secant are skipped.  SKIP_BN0: no p*
 // solve on faces without normal field (see below); with need_pstar false as
 // well, not even the HLL-state C2P whose total pressure would only feed the
-// p* output there (o.pstar is then 0).
+// p* output there (o.pstar is then 0).  INLINE_RES: the p* residual inlined
+// at its call sites (hlld_residual_at).
 template <int IDIR, typename T, typename TC = T, typename TP = T, bool IFT = false,
-          bool SKIP_BN0 = (sizeof(TC) == sizeof(float))>
+          bool SKIP_BN0 = (sizeof(TC) == sizeof(float)), bool INLINE_RES = false>
 __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, bool want_u,
                                           FaceOut<T> &o, const double *given = nullptr,
                                           bool need_pstar = true) {
@@ -1219,16 +1228,16 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         err = 0;
         iters_used = 0;
     } else {
-        TP f_lo = hlld_residual(C, p_lo);
-        TP f_hi = hlld_residual(C, p_hi);
+        TP f_lo = hlld_residual_at<INLINE_RES>(C, p_lo);
+        TP f_hi = hlld_residual_at<INLINE_RES>(C, p_hi);
         // bracket widening (hlld.py:1314-1321)
 #pragma unroll 1
         for (int w = 0; w < 5; ++w) {
             if (!((f_lo * f_hi) > TP(0))) break;
             p_lo = p_lo / TP(2);
             p_hi = p_hi * TP(2);
-            f_lo = hlld_residual(C, p_lo);
-            f_hi = hlld_residual(C, p_hi);
+            f_lo = hlld_residual_at<INLINE_RES>(C, p_lo);
+            f_hi = hlld_residual_at<INLINE_RES>(C, p_hi);
         }
 
         // clamped secant (hlld.py:669-746, _PSTAR_TOL hlld.py:1080, 30 iterations)
@@ -1248,7 +1257,7 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
             TP dx = safe ? f1 * (x1 - x0) / df : TP(0);
             TP x2 = x1 - dx;
             x2 = clamp_lo(x2, TP(1e-30));
-            TP f2 = hlld_residual(C, x2);
+            TP f2 = hlld_residual_at<INLINE_RES>(C, x2);
             x0 = x1;
             f0 = f1;
             x1 = x2;
