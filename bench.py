@@ -505,12 +505,7 @@ def _vortex_block(a, rp, dev):
         torch.cuda.empty_cache()
     n = a.vortex_n
     runs = {p: _stepper("vortex", n, p, dev) for p in ("fp64", "mixed")}
-    g, pert, sp = _stepper("vortex", n, "fp64", dev)
-    gen = torch.Generator(device=dev).manual_seed(1)
-    for k in ("D", "tau"):
-        noise = 2 * torch.rand(pert.cons[k].shape, generator=gen, device=dev, dtype=torch.float64) - 1
-        pert.cons[k].mul_(1 + 1e-13 * noise)
-    sp.sync(pert)
+    g, pert, sp = _perturbed_fp64("vortex", n, dev)
     t, steps = 0.0, 0
     while t < a.vortex_tend - 1e-14:
         dt = min(float(runs["fp64"][2].compute_dt(runs["fp64"][1], a.cfl).item()), a.vortex_tend - t)
@@ -1046,12 +1041,27 @@ def run_vortex(a):
     return 0
 
 
+def _perturbed_fp64(problem, n, dev):
+    """An FP64 stepper whose initial D and tau carry seeded relative noise of
+    1e-13, resynced: the spread of FP64 itself under round-off."""
+    import torch
+
+    g, pert, sp = _stepper(problem, n, "fp64", dev)
+    gen = torch.Generator(device=dev).manual_seed(1)
+    for k in ("D", "tau"):
+        noise = 2 * torch.rand(pert.cons[k].shape, generator=gen, device=dev, dtype=torch.float64) - 1
+        pert.cons[k].mul_(1 + 1e-13 * noise)
+    sp.sync(pert)
+    return g, pert, sp
+
+
 def run_rotor_whole(a):
     """Whole rotor runs from t = 0 to a.tend at a.n^2 in the mixed, FP32 and
     FP64 forms, all with the FP64 run's CFL dt sequence: each form's mean
     zone-updates/s over the run (CUDA events around every step, the dt
     computation of the FP64 run excluded) and the density L1/Linf of the
-    mixed and FP32 runs against FP64 at a.tend."""
+    mixed and FP32 runs against FP64 at a.tend, beside those of an untimed
+    FP64 run from an initial state perturbed by 1e-13."""
     import torch
 
     from hlld_ai_b200 import replicas
@@ -1061,6 +1071,7 @@ def run_rotor_whole(a):
     torch.cuda.set_device(rp.local)
     replicas.init(rp)
     runs = {p: _stepper(PROBLEM, a.n, p, dev) for p in ("fp64", "mixed", "fp32")}
+    _, pert, psp = _perturbed_fp64(PROBLEM, a.n, dev)
     stream = torch.cuda.current_stream(dev)
     ms = {p: 0.0 for p in runs}
     t, steps = 0.0, 0
@@ -1073,6 +1084,7 @@ def run_rotor_whole(a):
             e1.record(stream)
             e1.synchronize()
             ms[p] += e0.elapsed_time(e1)
+        psp.step(pert, dt, "rk3")
         t += dt
         steps += 1
     ph = runs["fp64"][0].phys
@@ -1085,6 +1097,8 @@ def run_rotor_whole(a):
         if p != "fp64":
             d = (runs[p][1].prims["rho"][ph].double() - ref).abs()
             out[p].update(l1_rho=float(d.mean()), linf_rho=float(d.max()))
+    d = (pert.prims["rho"][ph].double() - ref).abs()
+    out["fp64_perturbed_1e-13"] = {"l1_rho": float(d.mean()), "linf_rho": float(d.max())}
     replicas.finish(rp)
     if rp.rank == 0:
         print(json.dumps({"metric": "zone-updates/s", "value": out["mixed"]["value"],

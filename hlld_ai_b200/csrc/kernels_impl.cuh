@@ -52,6 +52,14 @@ constexpr int kThreads = 128;
 #ifndef HLLD_SWEEP_MIN_BLOCKS
 #define HLLD_SWEEP_MIN_BLOCKS 4
 #endif
+// HLLD_SWEEP_PARK = 1: the sweep's faces keep the values that only the HLLD
+// star states read again in shared memory during the p* solve (hlld_face's
+// PARK_STRIDE); float faces only (the FP64 slot would not fit the 48 KB of
+// static shared memory beside the tile)
+#ifndef HLLD_SWEEP_PARK
+#define HLLD_SWEEP_PARK 0
+#endif
+constexpr int kSweepPark = (HLLD_SWEEP_PARK && sizeof(R) == sizeof(float)) ? kThreads : 0;
 // The 2D sweeps and the tube kernel solve no p* on faces without normal
 // field (their HLLE fallback output does not depend on it), except in the
 // exact form, which keeps the reference's solver counters.
@@ -382,6 +390,7 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
     constexpr int NW = 2 * S + 2;
     constexpr int TR = SweepTile<AXIS, S>::ROWS, TC = SweepTile<AXIS, S>::COLS;
     __shared__ T tile[7][TR][TC];
+    __shared__ T park[kSweepPark > 0 ? kParkWords : 1][kThreads];
     const Grid &g = p.g;
     const int cols = AXIS == 0 ? g.nyt : g.nyt + 1;
     const int rows = AXIS == 0 ? g.nxt + 1 : g.nxt;
@@ -489,8 +498,9 @@ __global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(
         }
         FaceOut<T> o;
         if (SOLVER == HLLD_SOLVER_HLLD)
-            hlld_face<AXIS, T, RB, RS, false, kSkipBnZero, true>(PL, PR, (T)g.gamma, false, o,
-                                                                  nullptr, p.pstar_out != nullptr);
+            hlld_face<AXIS, T, RB, RS, false, kSkipBnZero, true, kSweepPark>(
+                PL, PR, (T)g.gamma, false, o, nullptr, p.pstar_out != nullptr,
+                &park[0][threadIdx.x]);
         else if (SOLVER == HLLD_SOLVER_HLLC)
             hllc_face<AXIS, T>(PL, PR, (T)g.gamma, false, o);
         else
@@ -1027,6 +1037,24 @@ __device__ __forceinline__ unsigned long long block_max_any(unsigned long long x
     return r;
 }
 
+// |vx| + v_fast of one cell (driver.py:77-127 compute_dt), as the bits of a
+// non-negative double (ordered like the values; NaN above every number)
+__device__ __forceinline__ unsigned long long tube_speed_bits(double rho, double eps, double vx,
+                                                              double vy, double vz, double Bx,
+                                                              double By, double Bz, double gamma) {
+    double pr, cs2;
+    eos_press_cs2(eps, rho, gamma, pr, cs2);
+    double v2 = vx * vx + vy * vy + vz * vz;
+    double W = 1.0 / sqrt(clamp_lo(1.0 - v2, 1e-10));
+    double B2 = Bx * Bx + By * By + Bz * Bz;
+    double vdotB = vx * Bx + vy * By + vz * Bz;
+    double b2 = (B2 + vdotB * vdotB) / (W * W);
+    double h = 1.0 + eps + pr / rho;
+    double v02 = cs2 + (b2 / (rho * h + b2)) * (1.0 - cs2);
+    double vf = sqrt(clamp_hi(clamp_lo(v02, 0.0), 1.0));
+    return abs_bits(fabs(vx) + vf);
+}
+
 // DRV = false: driver2d.rk_step on a ny = 1 grid; DRV = true: the 1D
 // driver's rk2_step (driver.py:192-236) and run loop (driver.py:388-412).
 template <int LIM, int SOLVER, bool DRV>
@@ -1082,42 +1110,27 @@ __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
         double t = 0.0;
         int steps = 0;
         const int nst = DRV ? 2 : (p.scheme == 3 ? 3 : 2);
+        // this thread's max of |vx| + v_fast (as bits) over the cells it
+        // updates; after the first step of the launch it comes from the last
+        // stage's primitives, still in registers
+        unsigned long long mloc = 0;
         while ((DRV ? t < p.tend : t < p.tend - 1e-14) && steps < p.max_steps) {
             // dt = (cfl dx) / max(|vx| + v_fast) over the physical cells
-            unsigned long long mloc = 0;
-            for (int c = ng + threadIdx.x; c < ng + L; c += blockDim.x) {
-                const int64_t ci = base + c;
-                double rho = p.P[P_RHO][ci], eps = p.P[P_EPS][ci];
-                double vx = p.P[P_VX][ci], vy = p.P[P_VY][ci], vz = p.P[P_VZ][ci];
-                double Bx = p.P[P_BX][ci], By = p.P[P_BY][ci], Bz = p.P[P_BZ][ci];
-                double pr, cs2;
-                eos_press_cs2(eps, rho, p.gamma, pr, cs2);
-                double v2 = vx * vx + vy * vy + vz * vz;
-                double W = 1.0 / sqrt(clamp_lo(1.0 - v2, 1e-10));
-                double B2 = Bx * Bx + By * By + Bz * Bz;
-                double vdotB = vx * Bx + vy * By + vz * Bz;
-                double b2 = (B2 + vdotB * vdotB) / (W * W);
-                double h = 1.0 + eps + pr / rho;
-                double v02 = cs2 + (b2 / (rho * h + b2)) * (1.0 - cs2);
-                double vf = sqrt(clamp_hi(clamp_lo(v02, 0.0), 1.0));
-                unsigned long long b = abs_bits(fabs(vx) + vf);
-                mloc = mloc > b ? mloc : b;
+            if (steps == 0) {
+                for (int c = ng + threadIdx.x; c < ng + L; c += blockDim.x) {
+                    const int64_t ci = base + c;
+                    const unsigned long long b = tube_speed_bits(
+                        p.P[P_RHO][ci], p.P[P_EPS][ci], p.P[P_VX][ci], p.P[P_VY][ci],
+                        p.P[P_VZ][ci], p.P[P_BX][ci], p.P[P_BY][ci], p.P[P_BZ][ci], p.gamma);
+                    mloc = mloc > b ? mloc : b;
+                }
             }
             double mx = __longlong_as_double((long long)block_max_any(mloc, red));
+            mloc = 0;
             if (DRV && p.light) mx = 1.0;  // driver.py:120-125
             double dt = isnan(mx) ? mx : (1.0 / clamp_lo(mx, 1e-14)) * (p.cfl * dx);
             if (dt > p.tend - t) dt = p.tend - t;
             if (!(dt > 0.0)) break;
-            // (each thread loads all it needs before its first store: the
-            // arrays may alias for all the compiler knows, so a load after a
-            // store would wait for it, one memory latency per variable)
-            for (int c = threadIdx.x; c < nt; c += blockDim.x) {
-                RS u[8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) u[k] = p.U[k][base + c];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) p.U0[k][base + c] = u[k];
-            }
             for (int st = 0; st < nst; ++st) {
                 const double *w = p.scheme == 3 ? kRK3d[st] : kRK2d[st];
                 const RS w0 = RS(w[0]), w1 = RS(w[1]), w2 = RS(w[2] * dt);
@@ -1138,12 +1151,18 @@ __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
                 // and of the primitives into the ghost cells next to an edge
                 for (int c = ng + threadIdx.x; c < ng + L; c += blockDim.x) {
                     const int64_t ci = base + c;
+                    // (each thread loads all it needs before its first store:
+                    // the arrays may alias for all the compiler knows, so a
+                    // load after a store would wait for it)
                     RS u0[8], u[8];
                     R fl[8], fr[8];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        u0[k] = p.U0[k][ci];
                         u[k] = p.U[k][ci];
+                        // the first stage starts the step: U0 is U, stored here
+                        // for the later stages (physical cells only; no stage
+                        // reads U0 in a ghost cell)
+                        u0[k] = st == 0 ? u[k] : p.U0[k][ci];
                         if (k != C_BX) {
                             fl[k] = Ft[tube_flux_slot(k)][c];
                             fr[k] = Ft[tube_flux_slot(k)][c + 1];
@@ -1180,9 +1199,26 @@ __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
                     RS Pd[NPRIM];
                     cons_to_prim<RS>(un, RS(p.gamma), RS(p.atmo_rho), RS(1e-10), Pd, nullptr, mu0);
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) p.U[k][ci] = un[k];
+                    for (int k = 0; k < 8; ++k) {
+                        if (st == 0 && nst > 1) p.U0[k][ci] = u[k];
+                        p.U[k][ci] = un[k];
+                    }
 #pragma unroll
                     for (int k = 0; k < NPRIM; ++k) p.P[k][ci] = (R)Pd[k];
+                    if (st == nst - 1) {
+                        // the next step's speed, from the primitives as stored:
+                        // read back through volatile loads, so that the values
+                        // are the rounded ones in memory (in registers, a
+                        // contracting build could fuse the C2P's last products
+                        // into the speed's sums)
+                        auto stored = [&](int k) -> double {
+                            return (double)*(const volatile R *)&p.P[k][ci];
+                        };
+                        const unsigned long long b = tube_speed_bits(
+                            stored(P_RHO), stored(P_EPS), stored(P_VX), stored(P_VY),
+                            stored(P_VZ), stored(P_BX), stored(P_BY), stored(P_BZ), p.gamma);
+                        mloc = mloc > b ? mloc : b;
+                    }
                     for (int side = 0; side < 2; ++side) {
                         if (c != (side == 0 ? ng : ng + L - 1)) continue;
                         const int g0 = side == 0 ? 0 : ng + L;

@@ -103,8 +103,11 @@ template <typename T> __device__ __forceinline__ T sdiv(T num, T den) {
 
 // Reciprocal by Newton's method on f(y) = 1/y - d, whose step
 // y <- y + y (1 - d y) squares the relative error: the hardware's
-// approximate reciprocal as the seed and three steps, which leave an error of
-// a few ulp.  Used by the mixed form's FP64 p* solve and cell C2P
+// approximate reciprocal as the seed and HLLD_NR_STEPS steps.  Two steps
+// leave at most 1 ulp against the correctly rounded 1.0 / d (measured on
+// B200 over 2^20 doubles spread across the domain and its two ends; one step
+// leaves thousands of ulp, and a third step made the mixed x sweep 3 %
+// slower for nothing).  Used by the mixed form's FP64 p* solve and cell C2P
 // (HLLD_NR_RCP), whose tolerances are far above it.
 //
 // Domain: finite d with 2^-1000 <= |d| < 2^1000.  The seed flushes to zero
@@ -117,12 +120,15 @@ template <typename T> __device__ __forceinline__ T sdiv(T num, T den) {
 // [1e-12, 1e20] and of 1 + mu |B~|^2 >= 1, which leaves the domain only for
 // |B~|^2 = B^2 / D above 1e300, not a finite physical state.  (A check of the
 // domain at every call made the mixed sweep 13 % slower, so there is none.)
+#ifndef HLLD_NR_STEPS
+#define HLLD_NR_STEPS 2
+#endif
 __device__ __forceinline__ double nr_rcp(double d) {
 #if defined(__CUDA_ARCH__)
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
 #pragma unroll
-    for (int k = 0; k < 3; ++k) y = fma(y, fma(-d, y, 1.0), y);
+    for (int k = 0; k < HLLD_NR_STEPS; ++k) y = fma(y, fma(-d, y, 1.0), y);
     return y;
 #else
     return 1.0 / d;
@@ -901,6 +907,9 @@ __device__ __forceinline__ void hllc_face(const T *PL, const T *PR, T gamma, boo
 // ── HLLD (hlld.py:366-605, :669-746, :1202-1543) ─────────────────────────
 
 // HLLDComputation R vectors (hlld.py:401-428), energy form
+// words of hlld_face's shared-memory slot (PARK_STRIDE > 0)
+constexpr int kParkWords = 5 * NCONS + 2;
+
 template <typename T> struct HlldR {
     T RSiL, RSiR, RS1L, RS1R, RS2L, RS2R;
     T RBiL, RBiR, RB1L, RB1R, RB2L, RB2R;
@@ -1084,14 +1093,15 @@ template <typename TP> __device__ __forceinline__ TP hlld_ift_root(const HlldR<T
 // p* output there (o.pstar is then 0).  INLINE_RES: the p* residual inlined
 // at its call sites (hlld_residual_at).
 template <int IDIR, typename T, typename TC = T, typename TP = T, bool IFT = false,
-          bool SKIP_BN0 = (sizeof(TC) == sizeof(float)), bool INLINE_RES = false>
+          bool SKIP_BN0 = (sizeof(TC) == sizeof(float)), bool INLINE_RES = false,
+          int PARK_STRIDE = 0>
 __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, bool want_u,
                                           FaceOut<T> &o, const double *given = nullptr,
-                                          bool need_pstar = true) {
+                                          bool need_pstar = true, T *park = nullptr) {
     constexpr int i = IDIR, t1 = (IDIR + 1) % 3, t2 = (IDIR + 2) % 3;
     Phys<T> ph;
     srmhd_fluxes<IDIR>(PL, PR, gamma, ph);
-    const T cm = ph.cmin, cx = ph.cmax;
+    T cm = ph.cmin, cx = ph.cmax;
     T fH[NCONS], uH[NCONS];
 #pragma unroll
     for (int k = 0; k < NCONS; ++k) {
@@ -1221,6 +1231,22 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         C.BnR = UiR[C_BX + i];
     }
 
+    // PARK_STRIDE > 0: the two sides' states and fluxes, the HLL flux and the
+    // wave speeds -- needed again only by the star states -- wait in the
+    // caller's shared-memory slot (park[k * PARK_STRIDE], k < kParkWords)
+    // during the p* solve instead of holding registers through it
+    if constexpr (PARK_STRIDE > 0) {
+#pragma unroll
+        for (int k = 0; k < NCONS; ++k) {
+            park[(0 * NCONS + k) * PARK_STRIDE] = ph.L.u[k];
+            park[(1 * NCONS + k) * PARK_STRIDE] = ph.L.f[k];
+            park[(2 * NCONS + k) * PARK_STRIDE] = ph.R.u[k];
+            park[(3 * NCONS + k) * PARK_STRIDE] = ph.R.f[k];
+            park[(4 * NCONS + k) * PARK_STRIDE] = fH[k];
+        }
+        park[(5 * NCONS + 0) * PARK_STRIDE] = cm;
+        park[(5 * NCONS + 1) * PARK_STRIDE] = cx;
+    }
     TP p_star;
     int32_t err = 30, iters_used = 30;
     if constexpr (IFT) {
@@ -1270,6 +1296,20 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         p_star = x1;
     }
 
+    if constexpr (PARK_STRIDE > 0) {
+        // (volatile: read back from the slot, not kept in registers)
+        const volatile T *pk = park;
+#pragma unroll
+        for (int k = 0; k < NCONS; ++k) {
+            ph.L.u[k] = pk[(0 * NCONS + k) * PARK_STRIDE];
+            ph.L.f[k] = pk[(1 * NCONS + k) * PARK_STRIDE];
+            ph.R.u[k] = pk[(2 * NCONS + k) * PARK_STRIDE];
+            ph.R.f[k] = pk[(3 * NCONS + k) * PARK_STRIDE];
+            fH[k] = pk[(4 * NCONS + k) * PARK_STRIDE];
+        }
+        cm = pk[(5 * NCONS + 0) * PARK_STRIDE];
+        cx = pk[(5 * NCONS + 1) * PARK_STRIDE];
+    }
     HlldV<TP> V;
     hlld_vars<true>(C, p_star, V);
 
