@@ -86,6 +86,9 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint interval")
     ap.add_argument("--tubes", type=int, default=4096)
+    ap.add_argument("--tube-shape", default=None,
+                    help="threads,CTAs-per-SM of the tubes workload's launch instead of the "
+                         "autotuner's pick (e.g. 512,1; for profiling a fixed shape)")
     ap.add_argument("--chunk", type=float, default=0.01,
                     help="tubes: simulated time every tube advances per step")
     ap.add_argument("--cpu-tubes", type=int, default=30, help="tubes of the CPU baseline sample")
@@ -350,23 +353,24 @@ def _l1_mixed_vs_fp64(a, dev, steps):
 
 
 # DRAM bytes (read + write) of one mixed-precision sweep launch measured by
-# ncu on the rotor at 1536^2 (x: 95.44 + 74.61 MB, y: 95.87 + 51.18 MB over
+# ncu on the rotor at 1536^2 (x: 95.15 + 50.72 MB, y: 95.58 + 44.71 MB over
 # 2,373,140 faces each; profiles/sweep_kernel_rotor1536_mixed_ncu.md), per
 # face; the 2048^2 launch is scaled by its faces
-_SWEEP_DRAM_BYTES_PER_FACE_MIXED = (170.05e6 + 147.05e6) / 2 / 2373140
+_SWEEP_DRAM_BYTES_PER_FACE_MIXED = (145.88e6 + 140.29e6) / 2 / 2373140
 # FP64-pipe instructions (warp level) of the same two launches, per face
-_SWEEP_FP64_INST_PER_FACE_MIXED = (126.13e6 + 10.01e6) / 2 / 2373140
+_SWEEP_FP64_INST_PER_FACE_MIXED = (111.30e6 + 6.84e6) / 2 / 2373140
 # FP64 issue rate of one B200 SM: 2 warp instructions per cycle (64 lanes;
-# the ncu capture's 126.1 M FP64 instructions at 35.0 % of peak sustained
-# over 637 us at 1965 MHz on 148 SMs give 1.94)
+# an earlier capture's 126.1 M FP64 instructions at 35.0 % of peak
+# sustained over 637 us at 1965 MHz on 148 SMs give 1.94)
 _FP64_WARP_INST_PER_SM_CYCLE = 2
 
 
 # DRAM bytes (read + write) of one mixed-precision tubes_kernel launch
-# measured by ncu (2048 seeded tubes, chunk 0.0005: 6.046 + 8.150 GB over
-# 2.129e7 cell-updates; profiles/tubes_kernel_2048tubes_ncu.md), per
-# cell-update; a launch is scaled by its updates
-_TUBES_DRAM_BYTES_PER_UPDATE_MIXED = (6.046e9 + 8.150e9) / 2.129e7
+# measured by ncu (2048 seeded tubes, chunk 0.0005, 512 threads x 148 CTAs:
+# 4.679 + 7.875 GB over 2.129e7 cell-updates;
+# profiles/tubes_kernel_2048tubes_ncu.md), per cell-update; a launch is
+# scaled by its updates
+_TUBES_DRAM_BYTES_PER_UPDATE_MIXED = (4.679e9 + 7.875e9) / 2.129e7
 
 
 def _sweep_traffic(a):
@@ -693,64 +697,36 @@ def run_ours(a):
     # end to end through the public API with host buffers
     e2e = None
     if not a.no_e2e:
-        host = {("cons", k): torch.empty_like(st.cons[k], device="cpu").pin_memory() for k in EVOLVED_KEYS}
-        host.update({("prims", k): torch.empty_like(st.prims[k], device="cpu").pin_memory() for k in PRIM_KEYS})
-        host[("Bxf", None)] = torch.empty_like(st.Bxf, device="cpu").pin_memory()
-        host[("Byf", None)] = torch.empty_like(st.Byf, device="cpu").pin_memory()
+        from hlld_ai_b200 import HostStepper2D
+        from hlld_ai_b200.physics.state import State2D
 
-        def dev_tensor(kind, k):
-            return st.cons[k] if kind == "cons" else st.prims[k] if kind == "prims" else getattr(st, kind)
-
-        for (kind, k), h in host.items():
-            h.copy_(dev_tensor(kind, k))
-        nbytes = sum(h.numel() * h.element_size() for h in host.values())
-        ke = max(2, min(a.steps, 5))
+        host = State2D(cons={k: st.cons[k].cpu().pin_memory() for k in EVOLVED_KEYS},
+                       Bxf=st.Bxf.cpu().pin_memory(), Byf=st.Byf.cpu().pin_memory(),
+                       prims={k: st.prims[k].cpu().pin_memory() for k in PRIM_KEYS})
+        hs = HostStepper2D(stepper, host)
+        h2d, d2h = hs.bytes_per_step()
+        ke = max(3, min(a.steps, 8))
         torch.cuda.synchronize(dev)
         replicas.barrier(rp)
-        # Every step copies the whole state (cons, faces, prims) from pinned
-        # host memory and the whole result back.  The two directions run on
-        # their own streams so that they overlap (full duplex): the copy-in
-        # of array j for step k + 1 starts as soon as the copy-out of array j
-        # from step k has landed in its host buffer, and the step waits for
-        # every copy-in.
-        items = list(host.items())
-        s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
-        out_done = [None] * len(items)
+        # Every step copies the whole state (faces, primitives, conserved
+        # arrays) from pinned host memory and the whole result back, through
+        # HostStepper2D: the copies run on their own streams, the step starts
+        # once the faces and primitives are in, and the copy-in of an array
+        # for step k + 1 follows the copy-out of the same array from step k.
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        s_in.wait_event(e0)
         for _ in range(ke):
-            in_done = []
-            for j, ((kind, k), h) in enumerate(items):
-                with torch.cuda.stream(s_in):
-                    if out_done[j] is not None:
-                        s_in.wait_event(out_done[j])
-                    dev_tensor(kind, k).copy_(h, non_blocking=True)
-                    ev = torch.cuda.Event()
-                    ev.record(s_in)
-                    in_done.append(ev)
-            for ev in in_done:
-                stream.wait_event(ev)
-            stepper.step(st, stepper.compute_dt(st, a.cfl), "rk3")
-            step_done = torch.cuda.Event()
-            step_done.record(stream)
-            s_out.wait_event(step_done)
-            for j, ((kind, k), h) in enumerate(items):
-                with torch.cuda.stream(s_out):
-                    h.copy_(dev_tensor(kind, k), non_blocking=True)
-                    ev = torch.cuda.Event()
-                    ev.record(s_out)
-                    out_done[j] = ev
-        for ev in out_done:
-            stream.wait_event(ev)
+            hs.step(a.cfl, "rk3")
+        hs.synchronize()
         e1.record(stream)
         torch.cuda.synchronize(dev)
         e2e_rate, ems = replicas.job_rate(rp, zones * ke, e0.elapsed_time(e1))
         e2e = {"value": e2e_rate, "unit": "zone-updates/s",
-               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "steps": ke, "path": "Stepper2D.step + compute_dt with pinned host state; copy-in and "
-                       "copy-out on their own streams, overlapped"}
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "steps": ke, "path": "HostStepper2D.step (Stepper2D.step + compute_dt) on a pinned "
+                       "host state; copies on their own streams, overlapped with the step"}
+        del hs, host
 
     # the adjoint's cost against the forward (the rotor gradient study: 512^2,
     # 200 FP64 SSP-RK3 steps, checkpoints every 20, J = sum w |B|^2 / 2)
@@ -861,7 +837,12 @@ def run_tubes(a):
     precision = "mixed" if a.precision == "mixed" else a.precision
     b = TubeBatch(states, limiter="weno5z", solver="hlld", scheme="rk3", precision=precision,
                   device=dev)
-    tuned = b.autotune(tend=a.chunk / 4, sample=1024)
+    if a.tube_shape:
+        threads, per_sm = (int(v) for v in a.tube_shape.split(","))
+        b.threads = threads
+        b.blocks = per_sm * torch.cuda.get_device_properties(dev).multi_processor_count
+    else:
+        b.autotune(tend=a.chunk / 4, sample=1024)
     g = b.capture(tend=a.chunk)
     b.reset()
     L = torch.as_tensor(states.lengths, dtype=torch.int64, device=dev)
@@ -944,7 +925,7 @@ def run_tubes(a):
             "vs_baseline": None, "dtype": "f32+f64" if precision == "mixed" else "f64",
             "data": "synthetic",
             "config": {"workload": TUBES_WORKLOAD, "tubes": a.tubes, "chunk": a.chunk,
-                       "precision": precision, "threads": tuned[0], "blocks": tuned[1],
+                       "precision": precision, "threads": b.threads, "blocks": b.blocks,
                        "total_cells": b.total_cells, "parallelism": f"replicas x{world}",
                        "l2": "state of the batch above L2 (~0.7 GB), no flush"},
             "e2e": e2e,

@@ -8,5 +8,6 @@ interfaces.  The kernels live in libhlld_b200.so (C ABI: include/hlld_b200.h);
 """
 from . import _lib
 from .physics import *  # noqa: F401,F403
+from .host_step import HostStepper2D  # noqa: F401
 
 __version__ = "0.1.0"

@@ -86,6 +86,9 @@ SIGNATURES = {
     "hlld_rk_step_ct": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC), _VP,
                                        ctypes.c_size_t, ctypes.c_double, _VP, ctypes.c_int, _VP,
                                        _VP]),
+    "hlld_rk_step_ct_events": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
+                                              _VP, ctypes.c_size_t, ctypes.c_double, _VP,
+                                              ctypes.c_int, _VP, _VP, _VP, _VP]),
     "hlld_rk_step_ct_static": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC),
                                               ctypes.c_double, _VP, ctypes.c_int, _VP, _VP]),
     "hlld_sync_state": (ctypes.c_int, [ctypes.POINTER(Grid2DC), ctypes.POINTER(State2DC), _VP,

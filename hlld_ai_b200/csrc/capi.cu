@@ -192,6 +192,13 @@ int hlld_step2d_scratch_bytes(const hlld_grid2d_t *g, size_t *bytes) {
 int hlld_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scratch,
                     size_t scratch_bytes, double dt_host, const double *dt_dev, int scheme,
                     hlld_step_diag_t *diag, void *stream) {
+    return hlld_rk_step_ct_events(g, s, scratch, scratch_bytes, dt_host, dt_dev, scheme, diag,
+                                  stream, nullptr, nullptr);
+}
+
+int hlld_rk_step_ct_events(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scratch,
+                           size_t scratch_bytes, double dt_host, const double *dt_dev, int scheme,
+                           hlld_step_diag_t *diag, void *stream, void *cons_in, void *cons_out) {
     int rc = check_grid(g);
     if (rc) return rc;
     if ((rc = check_state(s))) return rc;
@@ -205,14 +212,15 @@ int hlld_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scrat
     if (!dt_dev && !(dt_host == dt_host)) return fail(HLLD_ERR_INVALID, "dt is NaN");
     hlld_step_diag_t *d = diag ? diag : sc.diag;
     cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t ein = (cudaEvent_t)cons_in, eout = (cudaEvent_t)cons_out;
     if (g->precision == HLLD_FP64_EXACT)
-        hlld::v_exact::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
+        hlld::v_exact::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st, ein, eout);
     else if (g->precision == HLLD_MIXED)
-        hlld::v_mixed::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
+        hlld::v_mixed::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st, ein, eout);
     else if (g->precision == HLLD_FP32)
-        hlld::v_fp32::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
+        hlld::v_fp32::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st, ein, eout);
     else
-        hlld::v_fp64::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st);
+        hlld::v_fp64::launch_rk_step_ct(g, s, sc, dt_host, dt_dev, scheme, d, st, ein, eout);
     return check_launch("rk_step_ct");
 }
 

@@ -47,19 +47,24 @@ using R = HLLD_REAL;
 using RB = HLLD_BRACKET_REAL;
 using RS = HLLD_STATE_REAL;
 constexpr int kThreads = 128;
-// minimum resident blocks per SM requested for the sweep kernel (caps its
-// registers at 65536 / (kThreads * this))
-#ifndef HLLD_SWEEP_MIN_BLOCKS
-#define HLLD_SWEEP_MIN_BLOCKS 4
-#endif
 // HLLD_SWEEP_PARK = 1: the sweep's faces keep the values that only the HLLD
 // star states read again in shared memory during the p* solve (hlld_face's
 // PARK_STRIDE); float faces only (the FP64 slot would not fit the 48 KB of
 // static shared memory beside the tile)
 #ifndef HLLD_SWEEP_PARK
-#define HLLD_SWEEP_PARK 0
+#define HLLD_SWEEP_PARK 1
 #endif
 constexpr int kSweepPark = (HLLD_SWEEP_PARK && sizeof(R) == sizeof(float)) ? kThreads : 0;
+// minimum resident blocks per SM requested for the sweep kernel (caps its
+// registers at 65536 / (kThreads * this)); 0 picks per form: 5 with the
+// parked face state (96 registers), else 4 (128).  Measured on B200 (rotor
+// 2048^2, mixed step): 4 unparked 5.70 ms, 4 parked 5.45 ms, 5 parked
+// 5.34 ms; FP64 step: 4 13.26 ms, 5 14.43 ms.
+#ifndef HLLD_SWEEP_MIN_BLOCKS
+#define HLLD_SWEEP_MIN_BLOCKS 0
+#endif
+constexpr int kSweepMinBlocks =
+    HLLD_SWEEP_MIN_BLOCKS > 0 ? HLLD_SWEEP_MIN_BLOCKS : (kSweepPark > 0 ? 5 : 4);
 // The 2D sweeps and the tube kernel solve no p* on faces without normal
 // field (their HLLE fallback output does not depend on it), except in the
 // exact form, which keeps the reference's solver counters.
@@ -384,7 +389,7 @@ template <int AXIS, int S> struct SweepTile {
 };
 
 template <int AXIS, int LIM, int SOLVER, bool EMF_HLL>
-__global__ void __launch_bounds__(kThreads, HLLD_SWEEP_MIN_BLOCKS) sweep_kernel(const SweepParams p) {
+__global__ void __launch_bounds__(kThreads, kSweepMinBlocks) sweep_kernel(const SweepParams p) {
     using T = R;
     constexpr int S = Stencil<LIM>::S;
     constexpr int NW = 2 * S + 2;
@@ -1419,7 +1424,7 @@ static void launch_ghost_faces(const Grid &G, RS *Bxf, RS *Byf, cudaStream_t st)
 
 void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,
                        hlld_step_diag_t *diag, cudaStream_t st, double *mu_out, double *mu_warm,
-                       bool start_from_prims) {
+                       bool start_from_prims, cudaEvent_t after_cons) {
     Grid G = make_grid(g);
     RS *cons[6];
     for (int k = 0; k < 6; ++k) cons[k] = (RS *)s->cons[k];
@@ -1427,6 +1432,9 @@ void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t 
     for (int k = 0; k < 9; ++k) prims[k] = (R *)s->prims[k];
     launch_ghost_faces(G, (RS *)s->Bxf, (RS *)s->Byf, st);
     launch_ghost_cc<RS>(G, cons, 6, st);
+    // the conserved arrays and the faces are final here: the C2P and the
+    // primitive ghosts only read them
+    if (after_cons) cudaEventRecord(after_cons, st);
     C2PCellsParams cp = {};
     cp.g = G;
     for (int k = 0; k < 6; ++k) cp.U[k] = cons[k];
@@ -1510,9 +1518,12 @@ void launch_ct_update2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, const S
     ct_update_kernel<<<grid1d((int64_t)(G.nx + 1) * (G.ny + 1)), kThreads, 0, st>>>(up);
 }
 
+// cons_in (may be NULL): waited for before the first stage's update, the
+// first launch that reads the conserved cell arrays; cons_out (may be NULL):
+// recorded once the conserved arrays and the faces hold the step's result.
 void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,
                        double dt_host, const double *dt_dev, int scheme, hlld_step_diag_t *diag,
-                       cudaStream_t st) {
+                       cudaStream_t st, cudaEvent_t cons_in, cudaEvent_t cons_out) {
     const int nst = scheme == 3 ? 3 : 2;
     for (int stage = 0; stage < nst; ++stage) {
         // sweep counters and max |F_D| restart every stage; the CT scale is
@@ -1520,14 +1531,16 @@ void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Sc
         cudaMemsetAsync(diag, 0, sizeof(hlld_step_diag_t), st);
         launch_sweep2d(g, s, 0, sc.Fx, &diag->sweep[0], st);
         launch_sweep2d(g, s, 1, sc.Fy, &diag->sweep[1], st);
+        if (stage == 0 && cons_in) cudaStreamWaitEvent(st, cons_in, 0);
         launch_ct_update2d(g, s, sc, diag, stage, scheme, dt_host, dt_dev, st);
+        cudaEvent_t last = stage == nst - 1 ? cons_out : nullptr;
         // mixed form: stage 0 starts every cell's C2P root search from the
         // step's input primitives (mu = 1 / (h W)) and keeps the roots; the
         // later stages start from those (so a step depends on its input
         // state alone)
         if (stage == 0) launch_sync_state(g, s, nullptr, diag, st, sc.mu_warm, nullptr,
-                                            sc.mu_warm != nullptr);
-        else launch_sync_state(g, s, nullptr, diag, st, nullptr, sc.mu_warm);
+                                            sc.mu_warm != nullptr, last);
+        else launch_sync_state(g, s, nullptr, diag, st, nullptr, sc.mu_warm, false, last);
     }
 }
 

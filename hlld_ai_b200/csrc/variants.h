@@ -35,10 +35,12 @@ struct Scratch2D {
                              cudaStream_t st);                                                    \
     void launch_sync_state(const hlld_grid2d_t *g, const hlld_state2d_t *s, uint8_t *status,      \
                            hlld_step_diag_t *diag, cudaStream_t st, double *mu_out = nullptr,     \
-                           double *mu_warm = nullptr, bool start_from_prims = false);             \
+                           double *mu_warm = nullptr, bool start_from_prims = false,              \
+                           cudaEvent_t after_cons = nullptr);                                     \
     void launch_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, const Scratch2D &sc,  \
                            double dt_host, const double *dt_dev, int scheme,                      \
-                           hlld_step_diag_t *diag, cudaStream_t st);                              \
+                           hlld_step_diag_t *diag, cudaStream_t st,                               \
+                           cudaEvent_t cons_in = nullptr, cudaEvent_t cons_out = nullptr);        \
     void launch_compute_dt_2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, double cfl,        \
                               double *dt_dev, unsigned long long *work, cudaStream_t st);         \
     void launch_sweep2d(const hlld_grid2d_t *g, const hlld_state2d_t *s, int axis,                \

@@ -27,6 +27,17 @@ from .state import EVOLVED_KEYS, PRIM_KEYS, State2D, flat, unflat
 _SCHEMES = {"rk2": 2, "rk3": 3}
 
 
+def _event_handle(ev):
+    """The cudaEvent_t of a torch.cuda.Event (created on its first record or
+    wait), or None."""
+    if ev is None:
+        return None
+    h = ev.cuda_event
+    if not h:
+        raise ValueError("the event has not been recorded or waited on yet")
+    return h
+
+
 class Stepper2D:
     """Device resources and the C grid descriptor of one grid + option set."""
 
@@ -104,8 +115,14 @@ class Stepper2D:
                 state.prims[k] = t.to(self.prim_dtype).contiguous()
 
     # -- operations ---------------------------------------------------------
-    def step(self, state: State2D, dt, scheme: str = "rk3") -> None:
-        """One SSP-RK step in place.  dt: float, or a 1-element CUDA tensor."""
+    def step(self, state: State2D, dt, scheme: str = "rk3", cons_in=None, cons_out=None) -> None:
+        """One SSP-RK step in place.  dt: float, or a 1-element CUDA tensor.
+
+        cons_in / cons_out (torch.cuda.Event, optional; hlld_rk_step_ct_events):
+        the step waits for cons_in before its first read of the conserved
+        cell arrays, and records cons_out once the conserved arrays and the
+        faces hold its result -- for copies of the state that run on other
+        streams (HostStepper2D)."""
         s = self._struct(state)
         if isinstance(dt, torch.Tensor):
             if not dt.is_cuda or dt.dtype != torch.float64:
@@ -114,10 +131,17 @@ class Stepper2D:
         else:
             dt_host, dt_dev = float(dt), None
         with torch.cuda.device(self.device):
-            rc = _lib.lib().hlld_rk_step_ct(ctypes.byref(self.gc), ctypes.byref(s),
-                                            self._scratch_ptr, self.scratch_bytes, dt_host, dt_dev,
-                                            _SCHEMES[scheme], self.diag_buf.data_ptr(),
-                                            _lib.stream_handle(self.device))
+            if cons_in is None and cons_out is None:
+                rc = _lib.lib().hlld_rk_step_ct(ctypes.byref(self.gc), ctypes.byref(s),
+                                                self._scratch_ptr, self.scratch_bytes, dt_host,
+                                                dt_dev, _SCHEMES[scheme], self.diag_buf.data_ptr(),
+                                                _lib.stream_handle(self.device))
+            else:
+                rc = _lib.lib().hlld_rk_step_ct_events(
+                    ctypes.byref(self.gc), ctypes.byref(s), self._scratch_ptr, self.scratch_bytes,
+                    dt_host, dt_dev, _SCHEMES[scheme], self.diag_buf.data_ptr(),
+                    _lib.stream_handle(self.device), _event_handle(cons_in),
+                    _event_handle(cons_out))
         _lib.check(rc, "rk_step_ct")
 
     def sync(self, state: State2D, status: torch.Tensor | None = None) -> None:

@@ -212,6 +212,21 @@ int hlld_rk_step_ct(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scrat
                     size_t scratch_bytes, double dt_host, const double *dt_dev, int scheme,
                     hlld_step_diag_t *diag, void *stream);
 
+/* No counterpart in the reference.  hlld_rk_step_ct for a state whose arrays
+ * are copied between host and device memory on other streams while the step
+ * runs (a host-resident state stepped on the device).  cons_in (a
+ * cudaEvent_t, may be NULL): the stream waits for it before the first
+ * stage's update, the first launch that reads the conserved cell arrays; the
+ * primitives and the staggered field are read from the start, so they must
+ * be in place before the call's work begins.  cons_out (a cudaEvent_t, may
+ * be NULL) is recorded once the conserved arrays and the staggered field,
+ * ghosts included, hold the step's result: the last stage's C2P and the
+ * ghost fills of the primitives, which follow, read them but do not write
+ * them.  The arithmetic is hlld_rk_step_ct's, bit for bit. */
+int hlld_rk_step_ct_events(const hlld_grid2d_t *g, const hlld_state2d_t *s, void *scratch,
+                           size_t scratch_bytes, double dt_host, const double *dt_dev, int scheme,
+                           hlld_step_diag_t *diag, void *stream, void *cons_in, void *cons_out);
+
 /* No counterpart in the reference.  hlld_rk_step_ct for callers that cannot
  * allocate device memory: hosts whose device memory belongs to a pool or
  * allocator they do not control (a framework's caching allocator, a
