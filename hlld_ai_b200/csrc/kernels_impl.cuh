@@ -65,6 +65,14 @@ constexpr int kSweepPark = (HLLD_SWEEP_PARK && sizeof(R) == sizeof(float)) ? kTh
 #endif
 constexpr int kSweepMinBlocks =
     HLLD_SWEEP_MIN_BLOCKS > 0 ? HLLD_SWEEP_MIN_BLOCKS : (kSweepPark > 0 ? 5 : 4);
+// minimum resident blocks per SM requested for the cell C2P kernel: 8 (64
+// registers, a few spills) against the compiler's 96 registers at 5 blocks
+// measured on B200 (rotor 2048^2): mixed step 5.35 -> 5.22 ms, FP64 step
+// 13.30 -> 13.04 ms (6 blocks: 5.28 and 13.15 ms)
+#ifndef HLLD_C2P_MIN_BLOCKS
+#define HLLD_C2P_MIN_BLOCKS 8
+#endif
+constexpr int kC2PMinBlocks = HLLD_C2P_MIN_BLOCKS;
 // The 2D sweeps and the tube kernel solve no p* on faces without normal
 // field (their HLLE fallback output does not depend on it), except in the
 // exact form, which keeps the reference's solver counters.
@@ -778,7 +786,7 @@ __device__ __forceinline__ T kastaun_mu_of_prims(const R *const *P, int64_t c) {
 // overwrites (a template flag: a runtime one made the other launches 5 %
 // slower)
 template <bool FROM_PRIMS>
-__global__ void __launch_bounds__(kThreads) c2p_cells_kernel(const C2PCellsParams p) {
+__global__ void __launch_bounds__(kThreads, kC2PMinBlocks) c2p_cells_kernel(const C2PCellsParams p) {
     const Grid &g = p.g;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     Counts cnt = {};

@@ -1058,6 +1058,11 @@ template <typename T> __device__ __forceinline__ T hlld_residual(const HlldR<T> 
 // (INLINE = true; measured on B200: the mixed x sweep 1.084 -> 1.000 ms,
 // the FP64 one 2.62 -> 2.39 ms), out of line for the tube kernel, whose
 // phases share the instruction cache.
+// Which call sites of the p* solve inline the residual when INLINE_RES is
+// set: bit 0 the two bracket ends, bit 1 the widening, bit 2 the secant.
+#ifndef HLLD_RES_INLINE_SITES
+#define HLLD_RES_INLINE_SITES 7
+#endif
 template <bool INLINE, typename T> __device__ __forceinline__ T hlld_residual_at(const HlldR<T> &c, T p) {
     if constexpr (INLINE) return hlld_residual_body(c, p);
     else return hlld_residual(c, p);
@@ -1254,16 +1259,19 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         err = 0;
         iters_used = 0;
     } else {
-        TP f_lo = hlld_residual_at<INLINE_RES>(C, p_lo);
-        TP f_hi = hlld_residual_at<INLINE_RES>(C, p_hi);
+        constexpr bool kInB = INLINE_RES && (HLLD_RES_INLINE_SITES & 1);
+        constexpr bool kInW = INLINE_RES && (HLLD_RES_INLINE_SITES & 2);
+        constexpr bool kInS = INLINE_RES && (HLLD_RES_INLINE_SITES & 4);
+        TP f_lo = hlld_residual_at<kInB>(C, p_lo);
+        TP f_hi = hlld_residual_at<kInB>(C, p_hi);
         // bracket widening (hlld.py:1314-1321)
 #pragma unroll 1
         for (int w = 0; w < 5; ++w) {
             if (!((f_lo * f_hi) > TP(0))) break;
             p_lo = p_lo / TP(2);
             p_hi = p_hi * TP(2);
-            f_lo = hlld_residual_at<INLINE_RES>(C, p_lo);
-            f_hi = hlld_residual_at<INLINE_RES>(C, p_hi);
+            f_lo = hlld_residual_at<kInW>(C, p_lo);
+            f_hi = hlld_residual_at<kInW>(C, p_hi);
         }
 
         // clamped secant (hlld.py:669-746, _PSTAR_TOL hlld.py:1080, 30 iterations)
@@ -1283,7 +1291,7 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
             TP dx = safe ? f1 * (x1 - x0) / df : TP(0);
             TP x2 = x1 - dx;
             x2 = clamp_lo(x2, TP(1e-30));
-            TP f2 = hlld_residual_at<INLINE_RES>(C, x2);
+            TP f2 = hlld_residual_at<kInS>(C, x2);
             x0 = x1;
             f0 = f1;
             x1 = x2;
