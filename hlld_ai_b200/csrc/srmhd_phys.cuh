@@ -135,6 +135,38 @@ __device__ __forceinline__ double nr_rcp(double d) {
 #endif
 }
 
+// Square root by Newton's method (HLLD_NR_SQRT): the hardware's approximate
+// reciprocal square root y ~ 1/sqrt(x) as the seed, two steps of Newton on
+// g(y) = 1/y^2 - x, y <- y + (y/2)(1 - x y^2), then s = x y and one Newton
+// step on s^2 - x, s <- s + (y/2)(x - s^2).  For the mixed form's FP64 p*
+// residual and Kastaun master function, whose tolerances are far above its
+// error (checked against CUDA's correctly rounded sqrt on B200).  Domain: 0
+// (exactly 0 returned) and finite x with 2^-1000 <= x < 2^1000 (the seed
+// flushes outside it); a NaN gives a NaN.
+__device__ __forceinline__ double nr_sqrt(double x) {
+#if defined(__CUDA_ARCH__)
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double hy0 = 0.5 * y;
+    y = fma(hy0, fma(-x * y, y, 1.0), y);
+    const double hy1 = 0.5 * y;
+    y = fma(hy1, fma(-x * y, y, 1.0), y);
+    double sq = x * y;
+    sq = fma(0.5 * y, fma(-sq, sq, x), sq);
+    return x > 0.0 ? sq : x;
+#else
+    return sqrt(x);
+#endif
+}
+
+// sqrt of the mixed form's FP64 p* residual and master function
+template <typename T> __device__ __forceinline__ T sqrt_fast(T x) {
+#if defined(HLLD_NR_SQRT)
+    if constexpr (sizeof(T) == sizeof(double)) return nr_sqrt(x);
+#endif
+    return sqrt(x);
+}
+
 // 1 / x for the Kastaun master function: the Newton reciprocal in the mixed
 // form's FP64 cell C2P, a division everywhere else (the FP64 forms keep the
 // reference's quotients).
@@ -276,7 +308,7 @@ template <typename T> struct Kastaun {
         T qb = qbar(mu);
         T rb2 = rbar2(mu);
         T vhat2 = tmin((mu * mu) * rb2, v02);
-        const T sW = sqrt(clamp_lo(T(1) - vhat2, T(1e-10)));  // 1 / What
+        const T sW = sqrt_fast(clamp_lo(T(1) - vhat2, T(1e-10)));  // 1 / What
         T What = rcp_c2p(sW);
         T rhohat0 = kNewtonRcp<T> ? D * sW : D / What;
         T rhohat = tmin(tmax(rhohat0, T(1e-12)), T(1e15));
@@ -967,8 +999,8 @@ __device__ __forceinline__ void hlld_vars(const HlldR<T> &c, T p, HlldV<T> &o) {
     T waL = p + dAL(RTL - vRS_AL);
     T waR = p + dAR(RTR - vRS_AR);
 
-    T sqL = sqrt(clamp_lo(waL, T(0)));
-    T sqR = sqrt(clamp_lo(waR, T(0)));
+    T sqL = sqrt_fast(clamp_lo(waL, T(0)));
+    T sqR = sqrt_fast(clamp_lo(waR, T(0)));
 
     const T S_L = c.S_L, S_R = c.S_R;
     T dL = ncm * p + RTL - BnL * S_L * sqL;
@@ -1057,12 +1089,9 @@ template <typename T> __device__ __forceinline__ T hlld_residual(const HlldR<T> 
 // The residual at a p* solve's call sites: inlined for the 2D sweeps
 // (INLINE = true; measured on B200: the mixed x sweep 1.084 -> 1.000 ms,
 // the FP64 one 2.62 -> 2.39 ms), out of line for the tube kernel, whose
-// phases share the instruction cache.
-// Which call sites of the p* solve inline the residual when INLINE_RES is
-// set: bit 0 the two bracket ends, bit 1 the widening, bit 2 the secant.
-#ifndef HLLD_RES_INLINE_SITES
-#define HLLD_RES_INLINE_SITES 7
-#endif
+// phases share the instruction cache.  (Inlining only the secant's call,
+// with the bracket's and the widening's sharing one out-of-line body, was
+// slower in the sweep: 0.976 against 0.902 ms with everything inlined.)
 template <bool INLINE, typename T> __device__ __forceinline__ T hlld_residual_at(const HlldR<T> &c, T p) {
     if constexpr (INLINE) return hlld_residual_body(c, p);
     else return hlld_residual(c, p);
@@ -1259,19 +1288,16 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
         err = 0;
         iters_used = 0;
     } else {
-        constexpr bool kInB = INLINE_RES && (HLLD_RES_INLINE_SITES & 1);
-        constexpr bool kInW = INLINE_RES && (HLLD_RES_INLINE_SITES & 2);
-        constexpr bool kInS = INLINE_RES && (HLLD_RES_INLINE_SITES & 4);
-        TP f_lo = hlld_residual_at<kInB>(C, p_lo);
-        TP f_hi = hlld_residual_at<kInB>(C, p_hi);
+        TP f_lo = hlld_residual_at<INLINE_RES>(C, p_lo);
+        TP f_hi = hlld_residual_at<INLINE_RES>(C, p_hi);
         // bracket widening (hlld.py:1314-1321)
 #pragma unroll 1
         for (int w = 0; w < 5; ++w) {
             if (!((f_lo * f_hi) > TP(0))) break;
             p_lo = p_lo / TP(2);
             p_hi = p_hi * TP(2);
-            f_lo = hlld_residual_at<kInW>(C, p_lo);
-            f_hi = hlld_residual_at<kInW>(C, p_hi);
+            f_lo = hlld_residual_at<INLINE_RES>(C, p_lo);
+            f_hi = hlld_residual_at<INLINE_RES>(C, p_hi);
         }
 
         // clamped secant (hlld.py:669-746, _PSTAR_TOL hlld.py:1080, 30 iterations)
@@ -1291,7 +1317,7 @@ __device__ __forceinline__ void hlld_face(const T *PL, const T *PR, T gamma, boo
             TP dx = safe ? f1 * (x1 - x0) / df : TP(0);
             TP x2 = x1 - dx;
             x2 = clamp_lo(x2, TP(1e-30));
-            TP f2 = hlld_residual_at<kInS>(C, x2);
+            TP f2 = hlld_residual_at<INLINE_RES>(C, x2);
             x0 = x1;
             f0 = f1;
             x1 = x2;
