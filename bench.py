@@ -11,7 +11,8 @@ preceded by the on-device CFL time step, with the state resident in HBM
 C2P, p* iteration and RK state); the line also carries the FP64 step's rate
 and the mixed-vs-FP64 density L1/Linf after the timed number of steps (same
 dt sequence), the end-to-end rate through the public API with the state
-copied host -> device and back every step, the roofline of the dominant
+copied host -> device and back every step (HostStepper2D: the copies on
+their own streams, overlapped with the step), the roofline of the dominant
 kernel (the fused sweep), the CPU baseline (the C oracle on the host cores)
 and the SM clocks sampled during the timed region.
 
@@ -33,6 +34,13 @@ The default line also carries, each in its own block:
     kernel's roofline, and the density L1 against the oracle of a seeded
     subset advanced to t = 0.3;
   * ``adjoint``: the rotor gradient study's adjoint/forward cost.
+
+Workloads of their own (``--workload``): ``tubes`` (the tube block alone;
+``--tube-shape`` fixes the launch shape), ``adjoint``, ``vortex`` (the
+vortex block at --n / --vortex-n) and ``rotor_run`` (whole rotor runs to
+--tend in the mixed, FP32 and FP64 forms on the FP64 dt sequence, each
+form's mean rate and density L1/Linf against FP64, beside an untimed FP64
+run from a 1e-13-perturbed state).
 
 ``--impl reference`` times the CPU oracle (a C restatement of the
 reference's FP64 path) on the host cores with all threads, one RK3 step of

@@ -65,13 +65,6 @@ constexpr int kSweepPark = (HLLD_SWEEP_PARK && sizeof(R) == sizeof(float)) ? kTh
 #endif
 constexpr int kSweepMinBlocks =
     HLLD_SWEEP_MIN_BLOCKS > 0 ? HLLD_SWEEP_MIN_BLOCKS : (kSweepPark > 0 ? 5 : 4);
-// the y sweep's (0: the same as the x sweep's)
-#ifndef HLLD_SWEEP_Y_MIN_BLOCKS
-#define HLLD_SWEEP_Y_MIN_BLOCKS 0
-#endif
-template <int AXIS>
-constexpr int kSweepMinBlocksAxis =
-    (AXIS == 1 && HLLD_SWEEP_Y_MIN_BLOCKS > 0) ? HLLD_SWEEP_Y_MIN_BLOCKS : kSweepMinBlocks;
 // minimum resident blocks per SM requested for the cell C2P kernel: 8 (64
 // registers, a few spills) against the compiler's 96 registers at 5 blocks
 // measured on B200 (rotor 2048^2): mixed step 5.35 -> 5.22 ms, FP64 step
@@ -404,7 +397,7 @@ template <int AXIS, int S> struct SweepTile {
 };
 
 template <int AXIS, int LIM, int SOLVER, bool EMF_HLL>
-__global__ void __launch_bounds__(kThreads, kSweepMinBlocksAxis<AXIS>) sweep_kernel(const SweepParams p) {
+__global__ void __launch_bounds__(kThreads, kSweepMinBlocks) sweep_kernel(const SweepParams p) {
     using T = R;
     constexpr int S = Stencil<LIM>::S;
     constexpr int NW = 2 * S + 2;
