@@ -361,12 +361,12 @@ def _l1_mixed_vs_fp64(a, dev, steps):
 
 
 # DRAM bytes (read + write) of one mixed-precision sweep launch measured by
-# ncu on the rotor at 1536^2 (x: 95.15 + 50.72 MB, y: 95.58 + 44.71 MB over
+# ncu on the rotor at 1536^2 (x: 95.11 + 44.85 MB, y: 95.37 + 42.32 MB over
 # 2,373,140 faces each; profiles/sweep_kernel_rotor1536_mixed_ncu.md), per
 # face; the 2048^2 launch is scaled by its faces
-_SWEEP_DRAM_BYTES_PER_FACE_MIXED = (145.88e6 + 140.29e6) / 2 / 2373140
+_SWEEP_DRAM_BYTES_PER_FACE_MIXED = (139.96e6 + 137.69e6) / 2 / 2373140
 # FP64-pipe instructions (warp level) of the same two launches, per face
-_SWEEP_FP64_INST_PER_FACE_MIXED = (111.30e6 + 6.84e6) / 2 / 2373140
+_SWEEP_FP64_INST_PER_FACE_MIXED = (114.87e6 + 7.05e6) / 2 / 2373140
 # FP64 issue rate of one B200 SM: 2 warp instructions per cycle (64 lanes;
 # an earlier capture's 126.1 M FP64 instructions at 35.0 % of peak
 # sustained over 637 us at 1965 MHz on 148 SMs give 1.94)
