@@ -901,13 +901,24 @@ struct TubesParams {
     int smem_faces;  // faces whose seven fluxes fit the CTA's dynamic shared memory
 };
 
+// HLLD_TUBE_PARK = 1 (float faces): the tube kernel's faces keep the values
+// only the HLLD star states read again in a shared-memory slot during the
+// p* solve (hlld_face's PARK_STRIDE, here the kernel's 512-thread maximum),
+// at the front of the CTA's dynamic shared memory, before the fluxes
+#ifndef HLLD_TUBE_PARK
+#define HLLD_TUBE_PARK 1
+#endif
+constexpr int kTubeMaxThreads = 512;
+constexpr int kTubePark = (HLLD_TUBE_PARK && sizeof(R) == sizeof(float)) ? kTubeMaxThreads : 0;
+constexpr int kTubeParkBytes = kTubePark > 0 ? kParkWords * kTubeMaxThreads * (int)sizeof(R) : 0;
+
 // The seven flux slots of a tube face (F[Bx] = 0 is never stored): slot of
 // conserved component k
 __device__ __forceinline__ int tube_flux_slot(int k) { return k < C_BX ? k : k - 1; }
 
 template <int LIM, int SOLVER>
 __device__ __forceinline__ void tube_face(const TubesParams &p, int64_t base, int nt, int f,
-                                          R *const *Ft) {
+                                          R *const *Ft, R *park) {
     using T = R;
     constexpr int S = Stencil<LIM>::S;
     constexpr int NW = 2 * S + 2;
@@ -987,7 +998,8 @@ __device__ __forceinline__ void tube_face(const TubesParams &p, int64_t base, in
     }
     FaceOut<T> o;
     if (SOLVER == HLLD_SOLVER_HLLD)
-        hlld_face<0, T, RB, RS, false, kSkipBnZero>(PL, PR, (T)p.gamma, false, o, nullptr, false);
+        hlld_face<0, T, RB, RS, false, kSkipBnZero, false, kTubePark>(PL, PR, (T)p.gamma, false, o,
+                                                                        nullptr, false, park);
     else
         hlle_face<0, T>(PL, PR, (T)p.gamma, false, false, o);
 #pragma unroll
@@ -1106,7 +1118,7 @@ __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
             for (int k = 0; k < 8; ++k) {
                 if (k == C_BX) continue;
                 const int sl = tube_flux_slot(k);
-                Ft[sl] = in_smem ? reinterpret_cast<R *>(tube_smem) + (int64_t)sl * (nt + 1)
+                Ft[sl] = in_smem ? reinterpret_cast<R *>(tube_smem + kTubeParkBytes) + (int64_t)sl * (nt + 1)
                                  : p.F[k] + fbase;
             }
         }
@@ -1154,7 +1166,8 @@ __global__ void __launch_bounds__(512, 1) tubes_kernel(const TubesParams p) {
                         tube_face_driver1d<LIM, SOLVER>(p, base, nt, f, Ft);
                 } else {
                     for (int f = threadIdx.x; f <= nt; f += blockDim.x)
-                        tube_face<LIM, SOLVER>(p, base, nt, f, Ft);
+                        tube_face<LIM, SOLVER>(p, base, nt, f, Ft,
+                                               reinterpret_cast<R *>(tube_smem) + threadIdx.x);
                 }
                 __syncthreads();
                 // per physical cell: the update -- Heun (driver.py:223-232): U1 = U
@@ -1565,15 +1578,17 @@ static void tube_launch(K kernel, TubesParams tp, int blocks, int threads, cudaS
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     const int ctas_per_sm = (blocks + sms - 1) / (sms > 0 ? sms : 1);
-    int bytes = per_sm / (ctas_per_sm > 0 ? ctas_per_sm : 1) - 2048;  // static shared and reserve
+    // the parking slot first (always), then the fluxes in what the SM's
+    // share leaves
+    int bytes = per_sm / (ctas_per_sm > 0 ? ctas_per_sm : 1) - 2048 - kTubeParkBytes;
     if (bytes > kTubeSmemCap) bytes = kTubeSmemCap;
     if (bytes < 0) bytes = 0;
     tp.smem_faces = bytes / (7 * (int)sizeof(R));
-    bytes = tp.smem_faces * 7 * (int)sizeof(R);
+    bytes = kTubeParkBytes + tp.smem_faces * 7 * (int)sizeof(R);
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
         cudaGetLastError();  // clear it: fall back to the face arrays
         tp.smem_faces = 0;
-        bytes = 0;
+        bytes = kTubeParkBytes;
     }
     kernel<<<blocks, threads, bytes, st>>>(tp);
 }
