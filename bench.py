@@ -375,10 +375,10 @@ _FP64_WARP_INST_PER_SM_CYCLE = 2
 
 # DRAM bytes (read + write) of one mixed-precision tubes_kernel launch
 # measured by ncu (2048 seeded tubes, chunk 0.0005, 512 threads x 148 CTAs:
-# 4.679 + 7.875 GB over 2.129e7 cell-updates;
+# 3.329 + 6.225 GB over 2.129e7 cell-updates;
 # profiles/tubes_kernel_2048tubes_ncu.md), per cell-update; a launch is
 # scaled by its updates
-_TUBES_DRAM_BYTES_PER_UPDATE_MIXED = (4.679e9 + 7.875e9) / 2.129e7
+_TUBES_DRAM_BYTES_PER_UPDATE_MIXED = (3.329e9 + 6.225e9) / 2.129e7
 
 
 def _sweep_traffic(a):
